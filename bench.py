@@ -1,0 +1,379 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 short-range nonbonded path (tile-list build + force kernel).
+
+Workload: a 92,224-atom mixed system (30% seeded random-walk chains of 200
+atoms, 32 LJ types, 1-2/1-3 exclusions and scaled 1-4 pairs; the rest
+TIP3P-like water) in a 108 x 108 x 78 A periodic box; cutoff 12 A, switchdist
+10 A, pairlistdist 13.5 A, ewaldcof 0.2579. One step = one force + energy +
+virial evaluation (fast and slow buffers); tile lists are rebuilt and refined
+every 10 steps; coordinates follow a 100-frame trajectory in which every frame
+adds N(0, 0.02 A) noise to the previous one. The unit of work is one
+interacting pair (not excluded, r < 12 A), counted by the GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
+path does not shard. `--impl reference` times the CPU restatement of the
+reference's nonbonded evaluation on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "namd-3.0_b200"))
+
+METRIC = ("nonbonded pairs/s at 92k atoms (force err≤1e-5) vs plain GPU path & host CPU")
+UNIT = "pairs/s"
+FLOPS_PER_PAIR = 90          # algorithmic FP32 flops per interacting pair (FMA = 2)
+NATOMS, BOX, FRAC = 92224, (108.0, 108.0, 78.0), 0.3
+NFRAMES, REBUILD, SIGMA = 100, 10, 0.02
+WORKLOAD = ("mixed-92224: 92,224 atoms (30% random-walk chains + TIP3P-like water), "
+            "box 108x108x78 A, cutoff 12 / switch 10 / pairlist 13.5 A, ewaldcof 0.2579; "
+            "energy+virial+slow every eval; lists rebuilt every 10 evals; "
+            "100-frame trajectory with N(0,0.02 A) steps")
+PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "force_kernel_mixed92k.json")
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+def make_frames(seed: int):
+    """System, packing and the 100 frames of packed xyzq (host)."""
+    import nbk
+    sys_ = nbk.System(nbk.NBK_SYS_MIXED, seed, NATOMS, FRAC, box=BOX)
+    packed = nbk.Packed(sys_)
+    frames = np.empty((NFRAMES, packed.atomStorageSize, 4), dtype=np.float32)
+    frames[0] = packed.xyzq
+    for f in range(1, NFRAMES):
+        sys_.perturb(seed * 1000003 + f, SIGMA)
+        packed.update_positions()
+        frames[f] = packed.xyzq
+    return sys_, packed, frames
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def combine_ranks(total_ms: float, pairs: int, dist=None, device=None):
+    """Whole-job timing over replicas: the slowest rank's time and the pairs of
+    all ranks (every rank calls this at the same point)."""
+    if dist is None:
+        return total_ms, pairs
+    import torch
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    pc = torch.tensor([float(pairs)], dtype=torch.float64, device=device)
+    dist.all_reduce(pc, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(pc.item())
+
+
+# ---------------------------------------------------------------------------
+def cpu_eval_sample(packed, budget_s: float, max_evals: int = 1000):
+    """Times the CPU restatement (oracle/, all host threads) on whole evaluations
+    of the workload until `budget_s` is spent. Returns (pairs/s, threads, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import nbk
+    import oracle
+    o = oracle.Oracle(packed, nbk.NonbondedParams())
+    pairs, t0, n = 0, time.perf_counter(), 0
+    while n < max_evals:
+        pairs += o.eval_range(0, -1)
+        n += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return pairs / dt, oracle.num_threads(), f"{n} full evaluations (FP64, energies+virial) of frame 0"
+
+
+def run_reference(args, rank, world):
+    """The reference arm: CPU restatement of the nonbonded evaluation."""
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import nbk
+    import oracle
+    _, packed, frames = make_frames(2)
+    o = oracle.Oracle(packed, nbk.NonbondedParams())
+    nc = packed.numComputes
+    # size one step so that warmup + steps stay within ~2 minutes
+    t0 = time.perf_counter()
+    probe = max(1, nc // 16)
+    o.eval_range(0, probe)
+    t_per_compute = (time.perf_counter() - t0) / probe
+    budget = min(2.0, 120.0 / max(1, args.steps + args.warmup))
+    m = int(min(nc, max(1, budget / max(t_per_compute, 1e-9))))
+    pairs, total = 0, 0.0
+    for k in range(args.warmup + args.steps):
+        c0 = (k * m) % nc
+        c1 = min(nc, c0 + m)
+        t0 = time.perf_counter()
+        p = o.eval_range(c0, c1)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            pairs += p
+            total += dt
+    value = pairs / total
+    threads = oracle.num_threads()
+    sample = f"{m} of {nc} computes per step (FP64 restatement, all {threads} host threads)"
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---------------------------------------------------------------------------
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    import nbk
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    seed = 2 + 1000 * rank
+    t_setup = time.perf_counter()
+    sys_, packed, frames_h = make_frames(seed)
+    n = packed.atomStorageSize
+    params = nbk.NonbondedParams()
+    nb = nbk.Nonbonded(params, sys_.lj_table(), local_rank)
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+    nb.setup(packed, stream=st)
+    frames = torch.from_numpy(frames_h).to(dev)
+    dF = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    dS = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    dVE = torch.zeros(64, dtype=torch.float64, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    FL = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
+
+    def step(k):
+        f = k % NFRAMES
+        x = frames[f]
+        if k % REBUILD == 0:
+            nb.build_tile_lists(packed, xyzq=x, stream=st)
+            nb.force(packed, FL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS,
+                     stream=st)
+        else:
+            nb.force(packed, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+        nb.virial_energy_to(dVE.data_ptr(), True, stream=st)
+
+    # untimed pass over the trajectory: pairs per step (GPU-counted) + warm-up
+    pairs_of = np.zeros(NFRAMES, dtype=np.int64)
+    for k in range(NFRAMES):
+        step(k)
+        pairs_of[k] = nb.pair_count(st)
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize(dev)
+    log(f"[rank {rank}] setup {time.perf_counter() - t_setup:.1f}s, storage {n}, "
+        f"pairs/eval {pairs_of.mean():.4g}")
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[0])
+                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit()
+                           else local_rank)
+    launches0 = nb.launch_count()
+    nb.set_kernel_timing(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    time.sleep(0.1)
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()                     # L2 flush between timed steps (outside the events)
+        ev[k][0].record(stream)
+        step(k)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - wall0
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    launches = nb.launch_count() - launches0
+    ktimes = nb.kernel_times()
+    nb.set_kernel_timing(False)
+    step_ms = np.array([a.elapsed_time(b) for a, b in ev])
+    total_ms = float(step_ms.sum())
+    pairs = int(sum(pairs_of[k % NFRAMES] for k in range(args.steps)))
+    total_ms, pairs = combine_ranks(total_ms, pairs, dist, dev)
+    value = pairs / (total_ms * 1e-3)
+
+    # dominant kernel: steady-state force kernel (9 of every 10 launches)
+    steady = np.array([ktimes[k] for k in range(len(ktimes)) if k % REBUILD != 0])
+    plist = np.array([ktimes[k] for k in range(len(ktimes)) if k % REBUILD == 0])
+    steady_pairs = np.mean([pairs_of[k % NFRAMES] for k in range(args.steps) if k % REBUILD])
+    fp32_peak = nbk.measure_fp32_peak(local_rank)
+    achieved = FLOPS_PER_PAIR * steady_pairs / (steady.mean() * 1e-3) / 1e12
+    traffic = None
+    if os.path.exists(PROFILE_TRAFFIC):
+        try:
+            traffic = json.load(open(PROFILE_TRAFFIC)).get("dram_bytes_per_launch")
+        except (OSError, ValueError):
+            traffic = None
+    # algorithmic HBM bytes of one steady launch: xyzq + type read, fixed-point
+    # forces read-modified-written (6 x 8 B) per atom slot
+    alg_bytes = n * (16 + 4 + 2 * 48)
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak, "traffic": traffic,
+                "peak_source": "measured FP32 FMA loop on this GPU (nbk_measure_fp32_peak)",
+                "kernel": "forceKernel<energy,virial,slow> (steady state)",
+                "kernel_ms": float(steady.mean()), "pairlist_kernel_ms": float(plist.mean()) if len(plist) else None,
+                "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": float(steady_pairs),
+                "hbm_view": {"alg_bytes": alg_bytes,
+                             "achieved_gbs": alg_bytes / (steady.mean() * 1e-3) / 1e9}}
+
+    # e2e through the C-ABI with host buffers: H2D positions, D2H forces + energies
+    pin = torch.from_numpy(frames_h).pin_memory()
+    hF = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    hS = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    hVE = torch.empty(64, dtype=torch.float64).pin_memory()
+    ke = min(args.steps, 2 * NFRAMES)
+    eev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(ke)]
+
+    def step_e2e(k):
+        f = k % NFRAMES
+        x = pin[f].numpy()
+        if k % REBUILD == 0:
+            nb.build_tile_lists(packed, xyzq=x, stream=st)
+            nb.force(packed, FL | nbk.NBK_PAIRLIST, xyzq=None, d_forces=dF, d_forcesSlow=dS,
+                     h_forces=hF, h_forcesSlow=hS, stream=st)
+        else:
+            nb.force(packed, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, h_forces=hF,
+                     h_forcesSlow=hS, stream=st)
+        nb.virial_energy_to(hVE.data_ptr(), False, stream=st)
+
+    for k in range(3):
+        step_e2e(k)
+    torch.cuda.synchronize(dev)
+    for k in range(ke):
+        flush.zero_()
+        eev[k][0].record(stream)
+        step_e2e(k)
+        eev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in eev))
+    e2e_pairs = int(sum(pairs_of[k % NFRAMES] for k in range(ke)))
+    e2e_ms, e2e_pairs = combine_ranks(e2e_ms, e2e_pairs, dist, dev)
+    e2e = {"value": e2e_pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
+           "d2h_bytes_per_step": 2 * 16 * n + 8 * 31, "steps": ke}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, sample = cpu_eval_sample(packed, args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "atoms": NATOMS, "atom_slots": n,
+                       "pairs_per_eval": float(pairs_of.mean()), "rebuild_every": REBUILD,
+                       "l2": "flushed (512 MB write) between timed steps, outside the events",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "evals_per_s": args.steps / (total_ms * 1e-3) * world,
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(launches), "clocks": clocks,
+            "wall_s_timed_region": wall,
+        }
+        print(json.dumps(out))
+    nb.close()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

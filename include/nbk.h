@@ -1,0 +1,246 @@
+/*
+ * nbk.h — C-ABI of the B200 short-range nonbonded path (tile-list build +
+ * force kernel) that replaces NAMD 3.0's CudaTileListKernel /
+ * CudaComputeNonbondedKernel pair for one GPU.
+ *
+ * Every entry point:
+ *   - returns 0 on success or a negative NBK_ERR_* code; the message of the
+ *     last failure on the calling thread is returned by nbk_last_error().
+ *     Nothing here aborts the process (the reference calls NAMD_die /
+ *     cudaDie, src/CudaUtils.C:9-28, src/CudaUtils.h:214-221);
+ *   - takes the caller's CUDA stream (cudaStream_t passed as void*; NULL =
+ *     legacy default stream) and only enqueues work on it, except where a
+ *     comment says "synchronises";
+ *   - is NOT thread-safe per handle (the reference is called from masterPe
+ *     only, src/CudaComputeNonbonded.C:1090,1154,1607). Separate handles are
+ *     independent.
+ *
+ * Record layouts mirror the reference's structs field for field so a NAMD
+ * caller can hand its arrays over unchanged (see each struct's citation).
+ * Types are plain C: no CUDA or torch types appear in the signatures.
+ */
+#ifndef NBK_H
+#define NBK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NBK_API __attribute__((visibility("default")))
+
+/* ---- status codes --------------------------------------------------- */
+#define NBK_OK 0
+#define NBK_ERR_ARG (-1)       /* bad argument (null pointer, size, flag) */
+#define NBK_ERR_CUDA (-2)      /* a CUDA runtime call failed               */
+#define NBK_ERR_STATE (-3)     /* call out of order (e.g. force before build) */
+#define NBK_ERR_NOMEM (-4)     /* device or host allocation failed          */
+#define NBK_ERR_OVERFLOW (-5)  /* a size limit of the tile lists was exceeded */
+#define NBK_ERR_DEVICE (-6)    /* no usable sm_100 device                     */
+#define NBK_ERR_TIMEOUT (-7)   /* a bounded device-side wait gave up          */
+
+/* ---- flags for nbk_nonbonded_force / nbk_reduce_virial_energy -------- */
+#define NBK_ENERGY 1u      /* doEnergy   (src/CudaComputeNonbondedKernel.cu:2076) */
+#define NBK_VIRIAL 2u      /* doVirial */
+#define NBK_SLOW 4u        /* doSlow: PME real-space correction into the slow buffers */
+#define NBK_PAIRLIST 8u    /* doPairlist: refine tile lists to exclusion masks */
+#define NBK_CORRECTIONS 16u /* also apply excluded / modified (1-4) pair corrections
+                              (reference: ComputeBondedCUDAKernel exclusionForce /
+                              modifiedExclusionForce) in the same evaluation */
+
+/* ---- POD types -------------------------------------------------------- */
+typedef struct { float x, y, z; } nbk_float3;
+typedef struct { float x, y, z, w; } nbk_float4;     /* CudaAtom {x,y,z,q}: src/CudaRecord.h:58-60 */
+typedef struct { int x, y; } nbk_int2;
+
+/* CudaComputeRecord, src/CudaTileListKernel.h:47-50 (20 bytes). */
+typedef struct {
+  nbk_int2 patchInd;      /* (i-patch, j-patch) indices into the patch array */
+  nbk_float3 offsetXYZ;   /* i-shift in lattice units: center(pi)-center(pj)+image */
+} nbk_compute_record;
+
+/* CudaPatchRecord with NODEGROUP_FORCE_REGISTER, src/CudaTileListKernel.h:55-63. */
+typedef struct {
+  int numAtoms;
+  int numFreeAtoms;
+  int atomStart;          /* multiple of 32; padded slots repeat the last atom */
+  int patchID;
+} nbk_patch_record;
+
+/* TileList, src/CudaTileListKernel.h:10-22 (44 bytes). */
+typedef struct {
+  int iatomStart;
+  int jtileStart;
+  int jtileEnd;           /* inclusive */
+  nbk_float3 offsetXYZ;
+  nbk_int2 patchInd;
+  nbk_int2 patchNumList;
+  int icompute;
+} nbk_tile_list;
+
+/* TileExcl, src/CudaTileListKernel.h:5-8: bit t of excl[lane] = 1 iff the pair
+ * (i = iatomStart+lane, j = jatomStart+((lane+t)&31)) is within the pairlist
+ * cutoff and not excluded. */
+typedef struct { unsigned int excl[32]; } nbk_tile_excl;
+
+/* TileListStat, src/CudaTileListKernel.h:65-73 (bool widened to int). */
+typedef struct {
+  int numTileLists;
+  int numTileListsGBIS;
+  int numJtiles;
+  int numExcluded;
+  int patchReadyQueueCount;
+  int outputOrderIndex;
+  int tilesSizeExceeded;
+} nbk_tile_list_stat;
+
+/* VirialEnergy, src/CudaTileListKernel.h:98-117. virial[3*a+b] = sum F_a * x_b. */
+typedef struct {
+  double virial[9];
+  double virialSlow[9];
+  double energyVdw;
+  double energyElec;
+  double energySlow;
+  double energyVdw_s, energyElec_s, energySlow_s;          /* FEP: always 0 here */
+  double energyVdw_ti_1, energyVdw_ti_2;                   /* TI: always 0 here  */
+  double energyElec_ti_1, energyElec_ti_2;
+  double energySlow_ti_1, energySlow_ti_2;
+  double energyGBIS;                                       /* GBIS: always 0     */
+} nbk_virial_energy;
+
+/* CudaExclusion, src/TupleTypesCUDA.h:76-81. */
+typedef struct {
+  int i, j, vdwtypei, vdwtypej;
+  nbk_float3 ioffsetXYZ;  /* i-shift in lattice units */
+  int pswitch;            /* alchemical partition switch: must be 0 (no alchemy) */
+} nbk_exclusion;
+
+/* Nonbonded parameters: the ComputeNonbondedUtil statics the reference path
+ * reads (src/ComputeNonbondedUtil.C:506-576, src/CudaComputeNonbonded.C:
+ * 2318-2349) plus the LJ table that CudaNonbondedTables builds
+ * (src/CudaNonbondedTables.C:110-148). Arrays are host memory, copied. */
+typedef struct {
+  double cutoff;          /* cutoff (A) */
+  double switchdist;      /* switchdist (A); == cutoff disables switching */
+  double pairlistdist;    /* pairlistdist (A) */
+  double ewaldcof;        /* Ewald coefficient beta (1/A) */
+  double scaling;         /* nonbondedScaling */
+  double scale14;         /* 1-4scaling (1.0 unless exclude = scaled1-4) */
+  double slowScale;       /* fullElectFrequency / nonbondedFrequency */
+  int vdwTableDim;        /* number of LJ types */
+  const double* ljA;      /* [dim*dim] LJTable A   (unscaled) */
+  const double* ljB;      /* [dim*dim] LJTable B */
+  const double* ljA14;    /* [dim*dim] LJTable A for 1-4 pairs */
+  const double* ljB14;    /* [dim*dim] LJTable B for 1-4 pairs */
+} nbk_params;
+
+typedef struct nbk_context* nbk_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+NBK_API const char* nbk_last_error(void);
+NBK_API int nbk_version(void);
+
+/* CudaComputeNonbondedKernel(deviceID, CudaNonbondedTables&, doStreaming)
+ * (src/CudaComputeNonbondedKernel.h:86-135) + CudaTileListKernel(deviceID,
+ * doStreaming) (src/CudaTileListKernel.h:302) + CudaNonbondedTables(deviceID)
+ * (src/CudaNonbondedTables.C:10-34) in one handle. */
+NBK_API int nbk_create(int deviceID, const nbk_params* params, nbk_handle* out);
+NBK_API int nbk_destroy(nbk_handle h);
+
+/* ---- set-up (mirror of the reference's set-up calls) ------------------- */
+
+/* CudaTileListKernel::updateComputes, src/CudaTileListKernel.cu:893-902. */
+NBK_API int nbk_update_computes(nbk_handle h, int numComputes,
+                                const nbk_compute_record* h_computes, void* stream);
+
+/* CudaComputeNonbondedKernel::bindExclusions, src/CudaComputeNonbondedKernel.cu:3633-3639.
+ * bits: the exclusion bit array built by CudaComputeNonbonded::buildExclusions. */
+NBK_API int nbk_bind_exclusions(nbk_handle h, int numExclusions, const unsigned int* h_bits);
+
+/* CudaComputeNonbondedKernel::updateVdwTypesExcl, src/CudaComputeNonbondedKernel.cu:2038-2048.
+ * exclIndexMaxDiff[k] = (bit base, maxdiff) for slot k, as the reference. */
+NBK_API int nbk_update_vdw_types_excl(nbk_handle h, int atomStorageSize, const int* h_vdwTypes,
+                                      const nbk_int2* h_exclIndexMaxDiff, const int* h_atomIndex,
+                                      void* stream);
+
+/* ---- per-step work -------------------------------------------------------- */
+
+/* CudaTileListKernel::buildTileLists, src/CudaTileListKernel.cu:1022-1192.
+ * Bounding boxes per 32-atom tile and bbox culling of every compute into tile
+ * lists. xyzq is a host pointer (xyzqOnDevice = 0, copied on `stream`) or a
+ * device pointer kept by reference (xyzqOnDevice = 1; it must stay valid
+ * until the next build). No host synchronisation: capacities are exact upper
+ * bounds computed from the patch records. */
+NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSize,
+                                 int maxTileListLen, nbk_float3 lata, nbk_float3 latb,
+                                 nbk_float3 latc, const nbk_patch_record* h_patches,
+                                 const nbk_float4* xyzq, int xyzqOnDevice, float plcutoff2,
+                                 void* stream);
+
+/* CudaComputeNonbondedKernel::nonbondedForce, src/CudaComputeNonbondedKernel.cu:2076-3590.
+ * flags = NBK_ENERGY|NBK_VIRIAL|NBK_SLOW|NBK_PAIRLIST|NBK_CORRECTIONS.
+ * xyzq as for nbk_build_tile_lists (NULL = reuse the build's positions).
+ * Forces are accumulated deterministically as 64-bit fixed point (2^32 per
+ * kcal/mol/A) and then written as float4 to any non-NULL output:
+ *   d_forces / d_forcesSlow : device float4[atomStorageSize] (w = 0)
+ *   h_forces / h_forcesSlow : host float4[atomStorageSize], copied on `stream`
+ *   d_forcesFixed           : device int64[6*atomStorageSize] SoA
+ *                             (fx, fy, fz, fslowx, fslowy, fslowz)
+ * With NBK_PAIRLIST the tile lists are refined: masks of pairs within the
+ * pairlist cutoff that are not excluded, empty tiles and lists compacted. */
+NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flags,
+                                nbk_float3 lata, nbk_float3 latb, nbk_float3 latc,
+                                const nbk_float4* xyzq, int xyzqOnDevice, float cutoff2,
+                                nbk_float4* d_forces, nbk_float4* d_forcesSlow,
+                                nbk_float4* h_forces, nbk_float4* h_forcesSlow,
+                                long long* d_forcesFixed, void* stream);
+
+/* CudaComputeNonbondedKernel::reduceVirialEnergy, src/CudaComputeNonbondedKernel.cu:3595-3631.
+ * Writes the energies and virials of the last nbk_nonbonded_force into
+ * ve (device pointer if veOnDevice, else host pointer copied on `stream`). */
+NBK_API int nbk_reduce_virial_energy(nbk_handle h, unsigned flags, nbk_virial_energy* ve,
+                                     int veOnDevice, void* stream);
+
+/* Exclusion corrections of ComputeBondedCUDAKernel (modifiedExclusionForce,
+ * src/ComputeBondedCUDAKernel.cu:315-626; exclusionForce, :632-778): uploads
+ * the tuples; they are applied by every later nbk_nonbonded_force whose flags
+ * contain NBK_CORRECTIONS. modified = 1-4 pairs, excluded = full exclusions. */
+NBK_API int nbk_set_exclusion_tuples(nbk_handle h, int numModified, const nbk_exclusion* h_modified,
+                                     int numExcluded, const nbk_exclusion* h_excluded,
+                                     void* stream);
+
+/* CudaTileListKernel::reSortTileLists, src/CudaTileListKernel.cu:1605-1665.
+ * Compaction happens on the device inside nbk_nonbonded_force(NBK_PAIRLIST);
+ * this call only reads back the TileListStat and therefore synchronises. */
+NBK_API int nbk_get_tile_list_stat(nbk_handle h, nbk_tile_list_stat* out, void* stream);
+
+/* Test/debug export of the active tile lists (synchronises). Pass NULL
+ * arrays to query the counts first. */
+NBK_API int nbk_export_tile_lists(nbk_handle h, int* numTileLists, int* numJtiles,
+                                  nbk_tile_list* tileLists, int* tileJatomStart,
+                                  nbk_tile_excl* tileExcls, void* stream);
+
+/* ---- measurement ----------------------------------------------------------- */
+
+/* Enables (1) or disables (0) CUDA-event timing of every force-kernel launch
+ * of this handle; enabling clears the recorded launches. */
+NBK_API int nbk_set_kernel_timing(nbk_handle h, int enable);
+/* Durations (ms) of the force-kernel launches recorded since timing was
+ * enabled, oldest first (synchronises). *count receives the number recorded
+ * (at most 4096 are kept); at most maxCount are written. */
+NBK_API int nbk_get_kernel_times(nbk_handle h, float* ms, int maxCount, int* count);
+/* Pairs evaluated within the cutoff by the last nbk_nonbonded_force, which
+ * must have had NBK_ENERGY (the work unit of the pairs/s metric; synchronises). */
+NBK_API int nbk_get_pair_count(nbk_handle h, long long* pairs, void* stream);
+/* Number of kernels this handle has launched since it was created. */
+NBK_API long long nbk_launch_count(nbk_handle h);
+/* FP32 FMA throughput of the device (TFLOP/s, FMA = 2 flops), measured with a
+ * register-resident FMA loop over all SMs (synchronises; ~50 ms). */
+NBK_API int nbk_measure_fp32_peak(int deviceID, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NBK_H */

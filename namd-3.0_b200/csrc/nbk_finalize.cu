@@ -1,0 +1,227 @@
+// Excluded / modified pair corrections, the fixed-point -> float4 force
+// output with the per-atom part of the virial, and the energy/virial read-out.
+#include "nbk_internal.cuh"
+#include "nbk_launch.h"
+
+namespace nbk {
+
+// One thread per correction tuple (ComputeBondedCUDAKernel modifiedExclusionForce,
+// src/ComputeBondedCUDAKernel.cu:315-626, and exclusionForce, :632-778),
+// with r_ij = x_i + shift - x_j and analytic pair math in place of the tables.
+//   modified (1-4): LJ with (A14 - A, B14 - B); remove (1 - scale14) of the
+//     fast Coulomb and of the smooth (3 - r^2/rc^2)/(2 rc) part of the slow one
+//   excluded: slow -qq erf(beta r)/r
+// Both only within the cutoff, as the reference.
+template <bool doEnergy, bool doVirial, bool doSlow>
+__global__ void correctionsKernel(const CorrArgs a) {
+  const NbkConst& c = a.c;
+  const int total = a.numModified + (doSlow ? a.numExcluded : 0);
+  long long acc[kAccCount - 3] = {};  // energies + virials, thread-local
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    const bool modified = k < a.numModified;
+    const nbk_exclusion e = modified ? a.modified[k] : a.excluded[k - a.numModified];
+    const float3 sh = shiftOf(make_float3(e.ioffsetXYZ.x, e.ioffsetXYZ.y, e.ioffsetXYZ.z), a.lata,
+                              a.latb, a.latc);
+    const float4 xi = a.xyzq[e.i];
+    const float4 xj = a.xyzq[e.j];
+    // d = x_j - (x_i + shift): the nonbonded kernel's sign convention
+    const float dx = __fsub_rn(xj.x, __fadd_rn(xi.x, sh.x));
+    const float dy = __fsub_rn(xj.y, __fadd_rn(xi.y, sh.y));
+    const float dz = __fsub_rn(xj.z, __fadd_rn(xi.z, sh.z));
+    const float r2 = dist2(dx, dy, dz);
+    if (!(r2 < c.cutoff2)) continue;
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    const float rinv3 = rinv * rinv2;
+    const float qq = xi.w * xj.w;
+    float g = 0.f, gs = 0.f, eV = 0.f, eE = 0.f, eS = 0.f;
+    if (modified) {
+      const float2 ab = a.ljExclTable[e.vdwtypei * c.ljDim + e.vdwtypej];
+      const float rinv6 = rinv2 * rinv2 * rinv2;
+      const float ab6 = fmaf(ab.x, rinv6, -ab.y);
+      const float w = ab6 * rinv6;
+      const float dw = fmaf(ab.x, rinv6, ab6) * (-6.0f * rinv2 * rinv6);
+      float s = 1.0f, ds = 0.0f;
+      if (c.switching) {
+        const float t2 = fmaxf(r2, c.rs2);
+        const float d = c.rc2 - t2;
+        s = d * d * fmaf(c.lj1, t2, c.lj0);
+        ds = d * fmaf(c.lj2, t2, c.lj3);
+      }
+      const float q14 = c.one14 * qq;
+      g = fmaf(w, ds, dw * s) - q14 * (c.rc3inv - rinv3);
+      if (doEnergy) {
+        const float h = fmaf(c.hB, r2, c.hA);
+        eV = w * s;
+        eE = -q14 * (rinv - h);
+        if (doSlow) eS = -q14 * h;
+      }
+      if (doSlow) gs = q14 * c.rc3inv;
+    } else {
+      const float r = r2 * rinv;
+      const float x = c.beta * r;
+      const float erfx = erff(x);
+      gs = qq * (erfx * rinv3 - c.beta2Pi * __expf(-x * x) * rinv2);
+      if (doEnergy) eS = -qq * erfx * rinv;
+    }
+    // F_i += g d, F_j -= g d
+    const float fx = g * dx, fy = g * dy, fz = g * dz;
+    const unsigned long long qx = toFixedForce(fx), qy = toFixedForce(fy), qz = toFixedForce(fz);
+    if (modified) {
+      atomicAddFixed(&a.force[0 * (size_t)a.stride + e.i], qx);
+      atomicAddFixed(&a.force[1 * (size_t)a.stride + e.i], qy);
+      atomicAddFixed(&a.force[2 * (size_t)a.stride + e.i], qz);
+      atomicAddFixed(&a.force[0 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)qx));
+      atomicAddFixed(&a.force[1 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)qy));
+      atomicAddFixed(&a.force[2 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)qz));
+    }
+    unsigned long long sx = 0, sy = 0, sz = 0;
+    if (doSlow) {
+      sx = toFixedForce(gs * dx);
+      sy = toFixedForce(gs * dy);
+      sz = toFixedForce(gs * dz);
+      atomicAddFixed(&a.force[3 * (size_t)a.stride + e.i], sx);
+      atomicAddFixed(&a.force[4 * (size_t)a.stride + e.i], sy);
+      atomicAddFixed(&a.force[5 * (size_t)a.stride + e.i], sz);
+      atomicAddFixed(&a.force[3 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sx));
+      atomicAddFixed(&a.force[4 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sy));
+      atomicAddFixed(&a.force[5 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sz));
+    }
+    if (doEnergy) {
+      acc[kAccEVdw] += toFixedEnergy((double)eV);
+      acc[kAccEElec] += toFixedEnergy((double)eE);
+      acc[kAccESlow] += toFixedEnergy((double)eS);
+    }
+    if (doVirial) {
+      // shift part: F_i (x) shift; the per-atom part comes from the finalize pass
+      const double S[3] = {(double)sh.x, (double)sh.y, (double)sh.z};
+      const double Fi[3] = {(double)(long long)qx * kForceScaleInv,
+                            (double)(long long)qy * kForceScaleInv,
+                            (double)(long long)qz * kForceScaleInv};
+      const double Gi[3] = {(double)(long long)sx * kForceScaleInv,
+                            (double)(long long)sy * kForceScaleInv,
+                            (double)(long long)sz * kForceScaleInv};
+#pragma unroll
+      for (int p = 0; p < 9; ++p) {
+        if (modified) acc[kAccVir + p] += toFixedEnergy(Fi[p / 3] * S[p % 3]);
+        if (doSlow) acc[kAccVirSlow + p] += toFixedEnergy(Gi[p / 3] * S[p % 3]);
+      }
+    }
+  }
+  if (doEnergy || doVirial) {
+#pragma unroll
+    for (int p = 0; p < kAccCount - 3; ++p) {
+      long long v = warpSumLL(acc[p]);
+      if ((threadIdx.x & 31) == 0 && v != 0) atomicAddFixed(&a.acc[p], (unsigned long long)v);
+    }
+  }
+}
+
+cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st) {
+  const bool E = flags & NBK_ENERGY, V = flags & NBK_VIRIAL, S = flags & NBK_SLOW;
+  const int total = a.numModified + (S ? a.numExcluded : 0);
+  if (total <= 0) return cudaSuccess;
+  const int threads = 256;
+  const int blocks = min((total + threads - 1) / threads, 2048);
+  const int idx = (E ? 4 : 0) | (V ? 2 : 0) | (S ? 1 : 0);
+  switch (idx) {
+    case 0: correctionsKernel<false, false, false><<<blocks, threads, 0, st>>>(a); break;
+    case 1: correctionsKernel<false, false, true><<<blocks, threads, 0, st>>>(a); break;
+    case 2: correctionsKernel<false, true, false><<<blocks, threads, 0, st>>>(a); break;
+    case 3: correctionsKernel<false, true, true><<<blocks, threads, 0, st>>>(a); break;
+    case 4: correctionsKernel<true, false, false><<<blocks, threads, 0, st>>>(a); break;
+    case 5: correctionsKernel<true, false, true><<<blocks, threads, 0, st>>>(a); break;
+    case 6: correctionsKernel<true, true, false><<<blocks, threads, 0, st>>>(a); break;
+    case 7: correctionsKernel<true, true, true><<<blocks, threads, 0, st>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+// Fixed point -> float4 forces (transposeForcesKernel's role,
+// src/CudaComputeNonbondedKernel.cu:2057-2072) and the per-atom part of the
+// virial, sum_i F_i (x) x_i over patch-centred positions
+// (reduceNonbondedVirialKernel, :1649-1763), folded into fixed point per atom.
+__global__ void finalizeKernel(int n, const long long* __restrict__ F, int stride,
+                               const float4* __restrict__ xyzq, float4* __restrict__ outF,
+                               float4* __restrict__ outS, int doSlow, int doVirial,
+                               long long* __restrict__ acc) {
+  __shared__ long long s_v[32][18];
+  long long v[18] = {};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long long fx = F[i], fy = F[stride + i], fz = F[2 * (size_t)stride + i];
+    long long gx = 0, gy = 0, gz = 0;
+    if (doSlow) {
+      gx = F[3 * (size_t)stride + i];
+      gy = F[4 * (size_t)stride + i];
+      gz = F[5 * (size_t)stride + i];
+    }
+    if (outF)
+      outF[i] = make_float4((float)(fx * kForceScaleInv), (float)(fy * kForceScaleInv),
+                            (float)(fz * kForceScaleInv), 0.0f);
+    if (outS)
+      outS[i] = make_float4((float)(gx * kForceScaleInv), (float)(gy * kForceScaleInv),
+                            (float)(gz * kForceScaleInv), 0.0f);
+    if (doVirial) {
+      const float4 x = xyzq[i];
+      const double X[3] = {(double)x.x, (double)x.y, (double)x.z};
+      const double Fd[3] = {fx * kForceScaleInv, fy * kForceScaleInv, fz * kForceScaleInv};
+      const double Gd[3] = {gx * kForceScaleInv, gy * kForceScaleInv, gz * kForceScaleInv};
+#pragma unroll
+      for (int p = 0; p < 9; ++p) {
+        v[p] += toFixedEnergy(Fd[p / 3] * X[p % 3]);
+        v[9 + p] += toFixedEnergy(Gd[p / 3] * X[p % 3]);
+      }
+    }
+  }
+  if (!doVirial) return;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int p = 0; p < 18; ++p) {
+    const long long s = warpSumLL(v[p]);
+    if (lane == 0) s_v[w][p] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < 18) {
+    long long t = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += s_v[k][threadIdx.x];
+    if (threadIdx.x >= 9 && !doSlow) t = 0;
+    if (t != 0) atomicAddFixed(&acc[kAccVir + threadIdx.x], (unsigned long long)t);
+  }
+}
+
+cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
+                                 float4* outF, float4* outS, unsigned flags, long long* acc,
+                                 int numSM, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const bool V = flags & NBK_VIRIAL;
+  if (!V && !outF && !outS) return cudaSuccess;
+  const int threads = 256;
+  const int blocks = min((n + threads - 1) / threads, numSM * 4);
+  finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS,
+                                             (flags & NBK_SLOW) ? 1 : 0, V ? 1 : 0, acc);
+  return cudaGetLastError();
+}
+
+__global__ void energyVirialKernel(const long long* __restrict__ acc, nbk_virial_energy* out) {
+  const int t = threadIdx.x;
+  double* o = reinterpret_cast<double*>(out);
+  const int nd = (int)(sizeof(nbk_virial_energy) / sizeof(double));
+  if (t < nd) o[t] = 0.0;
+  __syncwarp();
+  if (t < 9) {
+    out->virial[t] = (double)acc[kAccVir + t] * kEnergyScaleInv;
+    out->virialSlow[t] = (double)acc[kAccVirSlow + t] * kEnergyScaleInv;
+  }
+  if (t == 0) {
+    out->energyVdw = (double)acc[kAccEVdw] * kEnergyScaleInv;
+    out->energyElec = (double)acc[kAccEElec] * kEnergyScaleInv;
+    out->energySlow = (double)acc[kAccESlow] * kEnergyScaleInv;
+  }
+}
+
+cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st) {
+  energyVirialKernel<<<1, 32, 0, st>>>(acc, out);
+  return cudaGetLastError();
+}
+
+}  // namespace nbk

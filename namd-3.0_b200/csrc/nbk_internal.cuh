@@ -1,0 +1,184 @@
+// Device-side types and the FP32 pair math of the B200 nonbonded path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "nbk.h"
+
+namespace nbk {
+
+constexpr int kWarp = 32;
+// Forces are accumulated as 64-bit fixed point with 2^32 units per kcal/mol/A.
+constexpr float kForceScale = 4294967296.0f;
+constexpr double kForceScaleInv = 1.0 / 4294967296.0;
+// Energies and virials are accumulated as 64-bit fixed point with 2^30 units.
+constexpr double kEnergyScale = 1073741824.0;
+constexpr double kEnergyScaleInv = 1.0 / 1073741824.0;
+
+// Slots of the 64-bit accumulator block (energies, virials, counters).
+enum AccSlot {
+  kAccEVdw = 0,
+  kAccEElec = 1,
+  kAccESlow = 2,
+  kAccVir = 3,       // 9 entries, virial[3*a+b]
+  kAccVirSlow = 12,  // 9 entries
+  kAccNumExcl = 21,  // number of excluded pairs within the pairlist cutoff
+  kAccNumPairs = 22, // pairs evaluated within the cutoff (energy evaluations only)
+  kAccCount = 24
+};
+
+// Constants of the energy-switched LJ and C1-split PME real-space pair math.
+// The switching constants follow CudaComputeNonbonded::getNonbondedCoef
+// (src/CudaComputeNonbonded.C:2318-2349): lj0 = c1(rc^2 - 3 rs^2), lj1 = 2 c1,
+// lj2 = -12 c1, lj3 = 12 c1 rs^2 with c1 = 1/(rc^2 - rs^2)^3.
+struct NbkConst {
+  float cutoff2;
+  float plcutoff2;
+  float rc2;          // == cutoff2, switching upper end
+  float rs2;          // switch distance^2
+  float lj0, lj1, lj2, lj3;
+  float rc3inv;       // 1/rc^3
+  float hA, hB;       // (3 - r^2/rc^2)/(2 rc) = hA + hB r^2
+  float beta;         // Ewald coefficient
+  float beta2Pi;      // 2 beta / sqrt(pi)
+  float one14;        // 1 - scale14
+  int ljDim;          // LJ table row length
+  int switching;      // 0 when switchdist >= cutoff (plain truncated LJ)
+};
+
+// Bounding box of one 32-atom tile: centre and half-widths.
+struct BBox {
+  float x, y, z, wx, wy, wz;
+};
+
+// Per-list patch-pair record (PatchPairRecord, src/CudaTileListKernel.h:24-29).
+struct PatchPair {
+  int iatomSize, iatomFreeSize, jatomSize, jatomFreeSize;
+};
+
+// Sparse-list descriptor built on the host for every (compute, i-tile).
+struct ListSeed {
+  int icompute;
+  int itile;       // i-tile index inside patch 1
+  int jcapStart;   // first j-tile slot reserved for this list
+  int pad;
+};
+
+// Shift of the i atoms, offset . lattice, with the reference's operand order
+// (src/CudaComputeNonbondedKernel.cu:720-722) made explicit as FMAs so that
+// host and device agree bit for bit.
+__device__ __forceinline__ float3 shiftOf(const float3 o, const float3 a, const float3 b,
+                                          const float3 c) {
+  float3 s;
+  s.x = __fmaf_rn(o.z, c.x, __fmaf_rn(o.y, b.x, __fmul_rn(o.x, a.x)));
+  s.y = __fmaf_rn(o.z, c.y, __fmaf_rn(o.y, b.y, __fmul_rn(o.x, a.y)));
+  s.z = __fmaf_rn(o.z, c.z, __fmaf_rn(o.y, b.z, __fmul_rn(o.x, a.z)));
+  return s;
+}
+
+// r^2 of d = xj - xi with the operand order dx*dx + dy*dy + dz*dz contracted
+// left to right (src/CudaComputeNonbondedKernel.cu:1225-1230).
+__device__ __forceinline__ float dist2(float dx, float dy, float dz) {
+  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// FP32 pair math. f = (dE/dr)/r of LJ + fast electrostatics; fs = (dE/dr)/r
+// of the slow (PME real-space remainder) electrostatics. The caller applies
+// F_i += f (x_j - x_i), F_j -= f (x_j - x_i).
+//   LJ      E = (A r^-12 - B r^-6) S(r^2), S = 1 below rs, Hermite switch above
+//   fast    E = qq (1/r - (3 - r^2/rc^2)/(2 rc))
+//   slow    E = qq ((3 - r^2/rc^2)/(2 rc) + (erfc(beta r) - 1)/r)
+// (src/CudaComputeNonbondedInteractions.h:37-159 states the same forms.)
+template <bool doEnergy, bool doSlow>
+__device__ __forceinline__ void pairForce(const float r2, const float qq, const float2 ab,
+                                          const NbkConst& c, float& f, float& fs, float& eVdw,
+                                          float& eElec, float& eSlow) {
+  const float rinv = rsqrtf(r2);
+  const float rinv2 = rinv * rinv;
+  const float rinv6 = rinv2 * rinv2 * rinv2;
+  const float rinv3 = rinv * rinv2;
+  // switched LJ; t2 = max(r2, rs2) turns the switch off below rs exactly as
+  // the reference's branch does (S -> 1, dS -> 0 up to rounding)
+  const float ab6 = fmaf(ab.x, rinv6, -ab.y);           // A r^-6 - B
+  const float w = ab6 * rinv6;                           // A r^-12 - B r^-6
+  const float dw = fmaf(ab.x, rinv6, ab6) * (-6.0f * rinv2 * rinv6);  // (dw/dr)/r
+  float s = 1.0f, ds = 0.0f;
+  if (c.switching) {  // uniform over the grid
+    const float t2 = fmaxf(r2, c.rs2);
+    const float d = c.rc2 - t2;
+    s = d * d * fmaf(c.lj1, t2, c.lj0);
+    ds = d * fmaf(c.lj2, t2, c.lj3);
+  }
+  f = fmaf(w, ds, dw * s);
+  // fast electrostatics: qq (rc^-3 - r^-3)
+  f = fmaf(qq, c.rc3inv - rinv3, f);
+  float h = 0.0f;
+  if (doEnergy) {
+    eVdw = fmaf(w, s, eVdw);
+    h = fmaf(c.hB, r2, c.hA);
+    eElec = fmaf(qq, rinv - h, eElec);
+  }
+  if (doSlow) {
+    const float r = r2 * rinv;
+    const float x = c.beta * r;
+    const float ex = __expf(-x * x);
+    const float ec = erfcf(x);
+    // slow (dE/dr)/r = qq ((1 - erfc - 2b/sqrt(pi) r e^{-x^2}) r^-3 - rc^-3)
+    const float corr = fmaf(c.beta2Pi * r, ex, ec);
+    fs = qq * fmaf(1.0f - corr, rinv3, -c.rc3inv);
+    if (doEnergy) eSlow = fmaf(qq, fmaf(ec - 1.0f, rinv, h), eSlow);
+  } else {
+    fs = 0.0f;
+  }
+}
+
+__device__ __forceinline__ unsigned long long toFixedForce(float v) {
+  return (unsigned long long)__float2ll_rn(v * kForceScale);
+}
+
+__device__ __forceinline__ long long toFixedEnergy(double v) {
+  return __double2ll_rn(v * kEnergyScale);
+}
+
+__device__ __forceinline__ void atomicAddFixed(long long* p, unsigned long long v) {
+  atomicAdd(reinterpret_cast<unsigned long long*>(p), v);
+}
+
+__device__ __forceinline__ long long warpSumLL(long long v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warpSumD(double v) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---- kernel argument blocks ---------------------------------------------------
+struct ForceArgs {
+  const nbk_tile_list* lists;
+  const int* numListsDev;      // device count (compacted lists) or NULL
+  int numListsHost;            // used when numListsDev == NULL
+  const int* tileJatomStart;
+  nbk_tile_excl* tileExcls;    // read (steady) / written (pairlist)
+  int* jtileActive;            // pairlist: written
+  int* listActive;             // pairlist: number of active j-tiles per list
+  const PatchPair* patchPairs; // pairlist
+  const float4* xyzq;
+  const int* vdwTypes;
+  const int* atomIndex;
+  const int2* exclIndexMaxDiff;
+  const unsigned* exclBits;
+  int numExclWords;
+  const float2* ljTable;       // [ljDim*ljDim] (A, B) * scaling
+  float3 lata, latb, latc;
+  NbkConst c;
+  long long* force;            // SoA [6][stride] fixed point
+  int stride;
+  long long* acc;              // [kAccCount]
+};
+
+}  // namespace nbk

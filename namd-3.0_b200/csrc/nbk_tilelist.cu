@@ -1,0 +1,190 @@
+// Tile-list build of the B200 nonbonded path: tile bounding boxes, bbox
+// culling of every (compute, i-tile) into a j-tile list, and the compaction
+// that follows the pairlist refinement.
+//
+// The reference (src/CudaTileListKernel.cu:1022-1192) culls with one thread
+// per i-tile looping over the partner patch's tiles, allocates output with
+// atomics and re-launches after a host synchronisation when its buffer
+// overflows. Here one warp culls one i-tile (its lanes test 32 j-tiles at a
+// time, ballot + popc place the survivors), and every list writes into a
+// slot range reserved on the host from the patch sizes, so the build never
+// overflows, never synchronises with the host and can be captured in a graph.
+#include "nbk_internal.cuh"
+#include "nbk_launch.h"
+
+namespace nbk {
+
+// One warp per 32-atom tile: min/max reduction over the tile's atoms
+// (buildBoundingBoxesKernel, src/CudaTileListKernel.cu:242-281).
+__global__ void bboxKernel(int numTiles, const float4* __restrict__ xyzq, BBox* __restrict__ bb) {
+  const int lane = threadIdx.x & 31;
+  const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < numTiles; t += warpsPerGrid) {
+    const float4 x = xyzq[(size_t)t * 32 + lane];
+    float lx = x.x, ly = x.y, lz = x.z, hx = x.x, hy = x.y, hz = x.z;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+      lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+      ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+      lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+      hx = fmaxf(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+      hy = fmaxf(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+      hz = fmaxf(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+    }
+    if (lane == 0) {
+      BBox b;
+      b.x = 0.5f * (lx + hx);
+      b.y = 0.5f * (ly + hy);
+      b.z = 0.5f * (lz + hz);
+      b.wx = 0.5f * (hx - lx);
+      b.wy = 0.5f * (hy - ly);
+      b.wz = 0.5f * (hz - lz);
+      bb[t] = b;
+    }
+  }
+}
+
+// Lower bound of the distance^2 between two boxes (src/CudaTileListKernel.cu:286-292).
+__device__ __forceinline__ float bbDist2(const BBox& a, const BBox& b) {
+  const float dx = fmaxf(0.0f, fabsf(a.x - b.x) - a.wx - b.wx);
+  const float dy = fmaxf(0.0f, fabsf(a.y - b.y) - a.wy - b.wy);
+  const float dz = fmaxf(0.0f, fabsf(a.z - b.z) - a.wz - b.wz);
+  return dx * dx + dy * dy + dz * dz;
+}
+
+// One warp per (compute, i-tile): j tiles of the partner patch whose box is
+// within the pairlist cutoff (self computes: j-tile >= i-tile).
+__global__ void buildListsKernel(int numLists, const ListSeed* __restrict__ seeds,
+                                 const nbk_compute_record* __restrict__ computes,
+                                 const nbk_patch_record* __restrict__ patches,
+                                 const BBox* __restrict__ bb, float3 lata, float3 latb, float3 latc,
+                                 float cull2, nbk_tile_list* __restrict__ lists,
+                                 PatchPair* __restrict__ pp, int* __restrict__ tileJatomStart) {
+  const int lane = threadIdx.x & 31;
+  const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+  for (int L = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; L < numLists; L += warpsPerGrid) {
+    const ListSeed sd = seeds[L];
+    const nbk_compute_record cr = computes[sd.icompute];
+    const nbk_patch_record p1 = patches[cr.patchInd.x];
+    const nbk_patch_record p2 = patches[cr.patchInd.y];
+    const float3 sh = shiftOf(make_float3(cr.offsetXYZ.x, cr.offsetXYZ.y, cr.offsetXYZ.z), lata,
+                              latb, latc);
+    const bool zeroShift = !(dist2(sh.x, sh.y, sh.z) > 0.0f);
+    const bool self = zeroShift && (p1.atomStart == p2.atomStart);
+    BBox bi = bb[p1.atomStart / 32 + sd.itile];
+    bi.x += sh.x;
+    bi.y += sh.y;
+    bi.z += sh.z;
+    const int ntiles2 = (p2.numAtoms + 31) / 32;
+    int count = 0;
+    for (int k0 = 0; k0 < ntiles2; k0 += 32) {
+      const int k = k0 + lane;
+      bool pass = false;
+      if (k < ntiles2 && (!self || k >= sd.itile)) pass = bbDist2(bi, bb[p2.atomStart / 32 + k]) < cull2;
+      const unsigned ball = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        const int rank = __popc(ball & ((1u << lane) - 1u));
+        tileJatomStart[sd.jcapStart + count + rank] = p2.atomStart + k * 32;
+      }
+      count += __popc(ball);
+    }
+    if (lane == 0) {
+      nbk_tile_list t;
+      t.iatomStart = p1.atomStart + sd.itile * 32;
+      t.jtileStart = sd.jcapStart;
+      t.jtileEnd = sd.jcapStart + count - 1;
+      t.offsetXYZ = cr.offsetXYZ;
+      t.patchInd = cr.patchInd;
+      t.patchNumList.x = 0;
+      t.patchNumList.y = 0;
+      t.icompute = sd.icompute;
+      lists[L] = t;
+      PatchPair q;
+      q.iatomSize = p1.atomStart + p1.numAtoms;
+      q.iatomFreeSize = p1.atomStart + p1.numFreeAtoms;
+      q.jatomSize = p2.atomStart + p2.numAtoms;
+      q.jatomFreeSize = p2.atomStart + p2.numFreeAtoms;
+      pp[L] = q;
+    }
+  }
+}
+
+// After the pairlist refinement: drop j tiles without interacting pairs and
+// lists left empty (reSortTileLists' compaction, src/CudaTileListKernel.cu:
+// 1605-1665). counters[0] = lists kept, counters[1] = j tiles kept.
+__global__ void compactKernel(int numLists, const nbk_tile_list* __restrict__ src,
+                              const int* __restrict__ listActive, const int* __restrict__ jtileActive,
+                              const int* __restrict__ jatomSrc,
+                              const nbk_tile_excl* __restrict__ exclSrc,
+                              nbk_tile_list* __restrict__ dst, int* __restrict__ jatomDst,
+                              nbk_tile_excl* __restrict__ exclDst, int* __restrict__ counters) {
+  const int lane = threadIdx.x & 31;
+  const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
+  for (int L = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; L < numLists; L += warpsPerGrid) {
+    const int n = listActive[L];
+    if (n == 0) continue;
+    const nbk_tile_list s = src[L];
+    if (s.jtileEnd < s.jtileStart) continue;
+    int pos = 0, jpos = 0;
+    if (lane == 0) {
+      pos = atomicAdd(&counters[0], 1);
+      jpos = atomicAdd(&counters[1], n);
+    }
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+    jpos = __shfl_sync(0xffffffffu, jpos, 0);
+    int w = 0;
+    for (int j0 = s.jtileStart; j0 <= s.jtileEnd; j0 += 32) {
+      const int jt = j0 + lane;
+      const bool act = (jt <= s.jtileEnd) && jtileActive[jt];
+      unsigned ball = __ballot_sync(0xffffffffu, act);
+      if (act) jatomDst[jpos + w + __popc(ball & ((1u << lane) - 1u))] = jatomSrc[jt];
+      while (ball) {
+        const int b = __ffs(ball) - 1;
+        ball &= ball - 1;
+        exclDst[jpos + w].excl[lane] = exclSrc[j0 + b].excl[lane];
+        ++w;
+      }
+    }
+    if (lane == 0) {
+      nbk_tile_list d = s;
+      d.jtileStart = jpos;
+      d.jtileEnd = jpos + n - 1;
+      dst[pos] = d;
+    }
+  }
+}
+
+cudaError_t launchBBoxes(int numTiles, const float4* xyzq, BBox* bb, cudaStream_t st) {
+  if (numTiles <= 0) return cudaSuccess;
+  const int threads = 256;
+  const int blocks = min((numTiles + 7) / 8, 4096);
+  bboxKernel<<<blocks, threads, 0, st>>>(numTiles, xyzq, bb);
+  return cudaGetLastError();
+}
+
+cudaError_t launchBuildLists(int numLists, const ListSeed* seeds,
+                             const nbk_compute_record* computes, const nbk_patch_record* patches,
+                             const BBox* bb, float3 lata, float3 latb, float3 latc, float cull2,
+                             nbk_tile_list* lists, PatchPair* pp, int* tileJatomStart,
+                             cudaStream_t st) {
+  if (numLists <= 0) return cudaSuccess;
+  const int threads = 256;
+  const int blocks = min((numLists + 7) / 8, 8192);
+  buildListsKernel<<<blocks, threads, 0, st>>>(numLists, seeds, computes, patches, bb, lata, latb,
+                                               latc, cull2, lists, pp, tileJatomStart);
+  return cudaGetLastError();
+}
+
+cudaError_t launchCompact(int numLists, const nbk_tile_list* src, const int* listActive,
+                          const int* jtileActive, const int* jatomSrc, const nbk_tile_excl* exclSrc,
+                          nbk_tile_list* dst, int* jatomDst, nbk_tile_excl* exclDst, int* counters,
+                          int numSM, cudaStream_t st) {
+  if (numLists <= 0) return cudaSuccess;
+  const int threads = 256;
+  const int blocks = min((numLists + 7) / 8, numSM * 8);
+  compactKernel<<<blocks, threads, 0, st>>>(numLists, src, listActive, jtileActive, jatomSrc,
+                                            exclSrc, dst, jatomDst, exclDst, counters);
+  return cudaGetLastError();
+}
+
+}  // namespace nbk

@@ -1,0 +1,42 @@
+"""The C-ABI libraries load without a GPU and export every declared entry point."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import nbk
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared(header):
+    txt = open(os.path.join(ROOT, "include", header)).read()
+    return sorted(set(re.findall(r"NBK_API\s+[\w\s\*]+?\b(nbk_\w+)\s*\(", txt)))
+
+
+@pytest.mark.parametrize("header,lib", [("nbk.h", "libnbk.so"), ("nbk_host.h", "libnbk_host.so")])
+def test_library_exports_every_declared_symbol(header, lib):
+    names = _declared(header)
+    assert len(names) >= 8
+    L = C.CDLL(os.path.join(ROOT, "namd-3.0_b200", lib))
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_errors_are_returned_not_raised():
+    L = nbk.dev_lib()
+    # NULL arguments are rejected with a status code and a message
+    assert L.nbk_create(0, None, None) == -1
+    assert b"NULL" in L.nbk_last_error()
+    assert L.nbk_update_computes(None, 0, None, None) == -1
+    assert L.nbk_destroy(None) == 0
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lj = (1, [1.0], [1.0], [1.0], [1.0])
+    with pytest.raises(nbk.NbkError):
+        nbk.Nonbonded(nbk.NonbondedParams(), lj)
