@@ -49,6 +49,10 @@ extern "C" {
 #define NBK_CORRECTIONS 16u /* also apply excluded / modified (1-4) pair corrections
                               (reference: ComputeBondedCUDAKernel exclusionForce /
                               modifiedExclusionForce) in the same evaluation */
+#define NBK_ENERGY_FP64 32u /* with NBK_ENERGY: electrostatic pair energies from FP64
+                              geometry and FP64 erfc, summed in FP64 (forces stay FP32).
+                              For energy totals that cancel to a small fraction of
+                              the sum of |pair energies|; about 2-3x slower. */
 
 /* ---- POD types -------------------------------------------------------- */
 typedef struct { float x, y, z; } nbk_float3;

@@ -62,6 +62,7 @@ struct nbk_context {
   int numSM = 148;
   nbk_params prm{};
   NbkConst c{};
+  NbkConst64 c64{};
   int ljDim = 0;
   DBuf<float2> ljTable, ljExclTable;
   DBuf<unsigned> exclBits;
@@ -96,7 +97,7 @@ struct nbk_context {
   DBuf<nbk_tile_list> lists2;
   DBuf<int> jatom2;
   DBuf<nbk_tile_excl> excl2;
-  DBuf<int> counters;  // [0] lists kept, [1] j tiles kept
+  DBuf<int> counters;  // [0] lists kept, [1] j tiles kept, [2] force-kernel work counter
   bool built = false;     // tile lists built (sparse)
   bool refined = false;   // compacted lists valid
   float3 lata{}, latb{}, latc{};
@@ -166,6 +167,23 @@ void computeConsts(nbk_context* h) {
   c.one14 = (float)(1.0 - p.scale14);
   c.ljDim = h->ljDim;
   c.switching = sw ? 1 : 0;
+  c.hAd = 1.5 / rc;
+  c.hBd = -0.5 / (rc * rc2);
+  c.betad = p.ewaldcof;
+  NbkConst64& k = h->c64;
+  k.rc2 = rc2;
+  k.rs2 = rs2;
+  k.lj0 = c1 * (rc2 - 3.0 * rs2);
+  k.lj1 = 2.0 * c1;
+  k.lj2 = -12.0 * c1;
+  k.lj3 = 12.0 * c1 * rs2;
+  k.rc3inv = 1.0 / (rc * rc2);
+  k.hA = 1.5 / rc;
+  k.hB = -0.5 / (rc * rc2);
+  k.beta = p.ewaldcof;
+  k.beta2Pi = 2.0 * p.ewaldcof / std::sqrt(M_PI);
+  k.one14 = 1.0 - p.scale14;
+  k.switching = sw ? 1 : 0;
 }
 
 int checkHandle(nbk_handle h, const char* fn) {
@@ -484,7 +502,7 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   int rc = checkHandle(h, "nbk_nonbonded_force");
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  if (flags & ~31u) return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: unknown flag bits");
+  if (flags & ~63u) return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: unknown flag bits");
   const bool pairlist = flags & NBK_PAIRLIST;
   if (!h->built) return setErr(NBK_ERR_STATE, "nbk_nonbonded_force: tile lists not built");
   if (!pairlist && !h->refined)
@@ -522,6 +540,9 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   a.force = h->force.p;
   a.stride = n;
   a.acc = h->acc.p;
+  a.workCounter = h->counters.p + 2;
+  a.c64 = h->c64;
+  NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
   if (pairlist) {
     a.lists = h->lists1.p;
     a.numListsDev = nullptr;
@@ -548,7 +569,7 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     NBK_CUDA(h->lists2.ensure(nl), "nbk_nonbonded_force");
     NBK_CUDA(h->jatom2.ensure(nj), "nbk_nonbonded_force");
     NBK_CUDA(h->excl2.ensure(nj), "nbk_nonbonded_force");
-    NBK_CUDA(cudaMemsetAsync(h->counters.p, 0, sizeof(int) * 4, st), "nbk_nonbonded_force");
+    NBK_CUDA(cudaMemsetAsync(h->counters.p, 0, sizeof(int) * 2, st), "nbk_nonbonded_force");
     NBK_CUDA(launchCompact(h->numLists, h->lists1.p, h->listActive.p, h->jtileActive.p, h->jatom1.p,
                            h->excl1.p, h->lists2.p, h->jatom2.p, h->excl2.p, h->counters.p,
                            h->numSM, st), "tile-list compaction");
@@ -573,6 +594,7 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     ca.force = h->force.p;
     ca.stride = n;
     ca.acc = h->acc.p;
+    ca.c64 = h->c64;
     NBK_CUDA(launchCorrections(ca, flags, st), "exclusion corrections");
     h->launches += 1;
   }

@@ -12,7 +12,7 @@ namespace nbk {
 //     fast Coulomb and of the smooth (3 - r^2/rc^2)/(2 rc) part of the slow one
 //   excluded: slow -qq erf(beta r)/r
 // Both only within the cutoff, as the reference.
-template <bool doEnergy, bool doVirial, bool doSlow>
+template <bool doEnergy, bool doVirial, bool doSlow, bool doE64>
 __global__ void correctionsKernel(const CorrArgs a) {
   const NbkConst& c = a.c;
   const int total = a.numModified + (doSlow ? a.numExcluded : 0);
@@ -61,7 +61,25 @@ __global__ void correctionsKernel(const CorrArgs a) {
       const float r = r2 * rinv;
       const float x = c.beta * r;
       const float erfx = erff(x);
-      gs = qq * (erfx * rinv3 - c.beta2Pi * __expf(-x * x) * rinv2);
+      // (dE/dr)/r of -qq erf(x)/r is qq (erf(x) - 2/sqrt(pi) x e^{-x^2}) / r^3. The
+      // bracket is O(x^3) and cancels badly at excluded-pair distances (O-H:
+      // x = 0.25), so below x = 0.5 it is taken from its Taylor series in x^2:
+      // 2/sqrt(pi) x sum_{n>=1} (-1)^{n+1} 2n x^{2n} / ((2n+1) n!).
+      float bracket;
+      if (x < 0.5f) {
+        const float y = x * x;
+        float q = 1.0f / 5400.0f;
+        q = fmaf(q, y, -1.0f / 780.0f);
+        q = fmaf(q, y, 1.0f / 132.0f);
+        q = fmaf(q, y, -1.0f / 27.0f);
+        q = fmaf(q, y, 1.0f / 7.0f);
+        q = fmaf(q, y, -2.0f / 5.0f);
+        q = fmaf(q, y, 2.0f / 3.0f);
+        bracket = 1.1283791671f * x * y * q;
+      } else {
+        bracket = erfx - c.beta2Pi * r * __expf(-x * x);
+      }
+      gs = qq * bracket * rinv3;
       if (doEnergy) eS = -qq * erfx * rinv;
     }
     // F_i += g d, F_j -= g d
@@ -87,12 +105,63 @@ __global__ void correctionsKernel(const CorrArgs a) {
       atomicAddFixed(&a.force[4 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sy));
       atomicAddFixed(&a.force[5 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sz));
     }
-    if (doEnergy) {
+    if (doE64) {
+      // FP64 mode: energies and the complete pair virial W = -g d (x) d in FP64
+      const double S0 = (double)e.ioffsetXYZ.x, S1 = (double)e.ioffsetXYZ.y,
+                   S2 = (double)e.ioffsetXYZ.z;
+      const double d[3] = {
+          (double)xj.x - ((double)xi.x + (S0 * a.lata.x + S1 * a.latb.x + S2 * a.latc.x)),
+          (double)xj.y - ((double)xi.y + (S0 * a.lata.y + S1 * a.latb.y + S2 * a.latc.y)),
+          (double)xj.z - ((double)xi.z + (S0 * a.lata.z + S1 * a.latb.z + S2 * a.latc.z))};
+      const double r2d = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
+      const double ri = rsqrt(r2d), ri2 = ri * ri, ri3 = ri * ri2;
+      const double qqd = (double)xi.w * (double)xj.w;
+      const NbkConst64& k = a.c64;
+      double gd = 0.0, gsd = 0.0, eVd = 0.0, eEd = 0.0, eSd = 0.0;
+      if (modified) {
+        const float2 ab = a.ljExclTable[e.vdwtypei * c.ljDim + e.vdwtypej];
+        const double ri6 = ri2 * ri2 * ri2;
+        const double ab6 = fma((double)ab.x, ri6, -(double)ab.y);
+        const double w = ab6 * ri6;
+        const double dw = fma((double)ab.x, ri6, ab6) * (-6.0 * ri2 * ri6);
+        double sw = 1.0, dsw = 0.0;
+        if (k.switching) {
+          const double t2 = fmax(r2d, k.rs2), dd = k.rc2 - t2;
+          sw = dd * dd * fma(k.lj1, t2, k.lj0);
+          dsw = dd * fma(k.lj2, t2, k.lj3);
+        }
+        const double q14 = k.one14 * qqd, h = fma(k.hB, r2d, k.hA);
+        gd = fma(w, dsw, dw * sw) - q14 * (k.rc3inv - ri3);
+        eVd = w * sw;
+        eEd = -q14 * (ri - h);
+        if (doSlow) {
+          eSd = -q14 * h;
+          gsd = q14 * k.rc3inv;
+        }
+      } else {
+        const double r = r2d * ri, x = k.beta * r, erfx = erf(x);
+        gsd = qqd * (erfx * ri3 - k.beta2Pi * exp(-x * x) * ri2);
+        eSd = -qqd * erfx * ri;
+      }
+      if (doEnergy) {
+        acc[kAccEVdw] += toFixedEnergy(eVd);
+        acc[kAccEElec] += toFixedEnergy(eEd);
+        acc[kAccESlow] += toFixedEnergy(eSd);
+      }
+      if (doVirial) {
+#pragma unroll
+        for (int p = 0; p < 9; ++p) {
+          const double dd = d[p / 3] * d[p % 3];
+          if (modified) acc[kAccVir + p] += toFixedEnergy(-gd * dd);
+          if (doSlow) acc[kAccVirSlow + p] += toFixedEnergy(-gsd * dd);
+        }
+      }
+    } else if (doEnergy) {
       acc[kAccEVdw] += toFixedEnergy((double)eV);
       acc[kAccEElec] += toFixedEnergy((double)eE);
       acc[kAccESlow] += toFixedEnergy((double)eS);
     }
-    if (doVirial) {
+    if (doVirial && !doE64) {
       // shift part: F_i (x) shift; the per-atom part comes from the finalize pass
       const double S[3] = {(double)sh.x, (double)sh.y, (double)sh.z};
       const double Fi[3] = {(double)(long long)qx * kForceScaleInv,
@@ -119,20 +188,30 @@ __global__ void correctionsKernel(const CorrArgs a) {
 
 cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st) {
   const bool E = flags & NBK_ENERGY, V = flags & NBK_VIRIAL, S = flags & NBK_SLOW;
+  const bool D = E && (flags & NBK_ENERGY_FP64);
   const int total = a.numModified + (S ? a.numExcluded : 0);
   if (total <= 0) return cudaSuccess;
   const int threads = 256;
   const int blocks = min((total + threads - 1) / threads, 2048);
-  const int idx = (E ? 4 : 0) | (V ? 2 : 0) | (S ? 1 : 0);
+  const int idx = (D ? 8 : 0) | (E ? 4 : 0) | (V ? 2 : 0) | (S ? 1 : 0);
   switch (idx) {
-    case 0: correctionsKernel<false, false, false><<<blocks, threads, 0, st>>>(a); break;
-    case 1: correctionsKernel<false, false, true><<<blocks, threads, 0, st>>>(a); break;
-    case 2: correctionsKernel<false, true, false><<<blocks, threads, 0, st>>>(a); break;
-    case 3: correctionsKernel<false, true, true><<<blocks, threads, 0, st>>>(a); break;
-    case 4: correctionsKernel<true, false, false><<<blocks, threads, 0, st>>>(a); break;
-    case 5: correctionsKernel<true, false, true><<<blocks, threads, 0, st>>>(a); break;
-    case 6: correctionsKernel<true, true, false><<<blocks, threads, 0, st>>>(a); break;
-    case 7: correctionsKernel<true, true, true><<<blocks, threads, 0, st>>>(a); break;
+#define NBK_CASE(i, e, v, s, d) \
+  case i:                       \
+    correctionsKernel<e, v, s, d><<<blocks, threads, 0, st>>>(a); \
+    break;
+    NBK_CASE(0, false, false, false, false)
+    NBK_CASE(1, false, false, true, false)
+    NBK_CASE(2, false, true, false, false)
+    NBK_CASE(3, false, true, true, false)
+    NBK_CASE(4, true, false, false, false)
+    NBK_CASE(5, true, false, true, false)
+    NBK_CASE(6, true, true, false, false)
+    NBK_CASE(7, true, true, true, false)
+    NBK_CASE(12, true, false, false, true)
+    NBK_CASE(13, true, false, true, true)
+    NBK_CASE(14, true, true, false, true)
+    NBK_CASE(15, true, true, true, true)
+#undef NBK_CASE
   }
   return cudaGetLastError();
 }
@@ -197,8 +276,11 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
   if (!V && !outF && !outS) return cudaSuccess;
   const int threads = 256;
   const int blocks = min((n + threads - 1) / threads, numSM * 4);
+  // the FP64 energy/virial mode accumulates complete pair virials instead
+  const bool atomVirial = V && !((flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64));
+  if (!atomVirial && !outF && !outS) return cudaSuccess;
   finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS,
-                                             (flags & NBK_SLOW) ? 1 : 0, V ? 1 : 0, acc);
+                                             (flags & NBK_SLOW) ? 1 : 0, atomVirial ? 1 : 0, acc);
   return cudaGetLastError();
 }
 

@@ -20,14 +20,15 @@ namespace nbk {
 constexpr int kForceWarps = 4;
 constexpr int kForceThreads = kForceWarps * kWarp;
 
-template <bool doEnergy, bool doVirial, bool doSlow, bool doPairlist>
-__global__ void __launch_bounds__(kForceThreads)
+constexpr int kForceMinBlocks = 8;  // caps registers at 64 -> 32 warps per SM
+
+template <bool doEnergy, bool doVirial, bool doSlow, bool doPairlist, bool doE64>
+__global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
   __shared__ int s_type[kForceWarps][kWarp];
   __shared__ int s_jidx[kForceWarps][kWarp];
-  __shared__ long long s_red[kForceWarps][kAccCount];
 
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -44,7 +45,13 @@ __global__ void __launch_bounds__(kForceThreads)
   int nexcl = 0;
   int npair = 0;  // interacting pairs seen by this lane (energy evaluations)
 
-  for (int L = blockIdx.x * kForceWarps + wib; L < numLists; L += gridDim.x * kForceWarps) {
+  // lists are handed out one at a time from a global counter, so warps that
+  // draw short lists keep working instead of idling at the end
+  for (;;) {
+    int L = 0;
+    if (lane == 0) L = atomicAdd(a.workCounter, 1);
+    L = __shfl_sync(0xffffffffu, L, 0);
+    if (L >= numLists) break;
     const nbk_tile_list tl = a.lists[L];
     if (tl.jtileEnd < tl.jtileStart) continue;  // empty (warp-uniform)
     const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
@@ -54,6 +61,14 @@ __global__ void __launch_bounds__(kForceThreads)
 
     const int iatom = tl.iatomStart + lane;
     float4 xi = a.xyzq[iatom];
+    // FP64 shifted i position (FP64 energy mode): the shift is formed in FP64
+    // from the FP32 offsets and lattice, without the FP32 rounding of sh
+    double xid = 0.0, yid = 0.0, zid = 0.0;
+    if (doE64) {
+      xid = (double)xi.x + ((double)off.x * a.lata.x + (double)off.y * a.latb.x + (double)off.z * a.latc.x);
+      yid = (double)xi.y + ((double)off.x * a.lata.y + (double)off.y * a.latb.y + (double)off.z * a.latc.y);
+      zid = (double)xi.z + ((double)off.x * a.lata.z + (double)off.y * a.latb.z + (double)off.z * a.latc.z);
+    }
     xi.x = __fadd_rn(xi.x, sh.x);
     xi.y = __fadd_rn(xi.y, sh.y);
     xi.z = __fadd_rn(xi.z, sh.z);
@@ -75,6 +90,7 @@ __global__ void __launch_bounds__(kForceThreads)
 
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fisx = 0.f, fisy = 0.f, fisz = 0.f;
     double eV = 0.0, eE = 0.0, eS = 0.0;
+    double wv[6] = {0, 0, 0, 0, 0, 0}, ws[6] = {0, 0, 0, 0, 0, 0};  // FP64 pair virials
     int activeTiles = 0;
 
     for (int jt = tl.jtileStart; jt <= tl.jtileEnd; ++jt) {
@@ -152,6 +168,27 @@ __global__ void __launch_bounds__(kForceThreads)
           const float2 ab = s_lj[ti + s_type[wib][j]];
           float f, fs;
           pairForce<doEnergy, doSlow>(r2, xi.w * xjj.w, ab, c, f, fs, eVt, eEt, eSt);
+          if (doE64) {
+            // electrostatic energies and the pair virials again in FP64 from
+            // FP64 geometry; the FP32 eEt/eSt are discarded in this mode
+            const double ex = (double)xjj.x - xid, ey = (double)xjj.y - yid,
+                         ez = (double)xjj.z - zid;
+            const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
+            double g, gs;
+            pairFP64<doSlow>(r2d, (double)xi.w * (double)xjj.w, (double)ab.x, (double)ab.y,
+                             a.c64, g, gs, eE, eS);
+            if (doVirial) {
+              const double d[3] = {ex, ey, ez};
+#pragma unroll
+              for (int u = 0, q = 0; u < 3; ++u)
+#pragma unroll
+                for (int v = u; v < 3; ++v, ++q) {
+                  const double dd = d[u] * d[v];
+                  wv[q] = fma(-g, dd, wv[q]);
+                  if (doSlow) ws[q] = fma(-gs, dd, ws[q]);
+                }
+            }
+          }
           const float fx = dx * f, fy = dy * f, fz = dz * f;
           fix += fx;
           fiy += fy;
@@ -195,8 +232,10 @@ __global__ void __launch_bounds__(kForceThreads)
       }
       if (doEnergy) {
         eV += (double)eVt;
-        eE += (double)eEt;
-        if (doSlow) eS += (double)eSt;
+        if (!doE64) {
+          eE += (double)eEt;
+          if (doSlow) eS += (double)eSt;
+        }
       }
       if (doPairlist) {
         a.tileExcls[jt].excl[lane] = newMask;
@@ -225,7 +264,24 @@ __global__ void __launch_bounds__(kForceThreads)
         atomicAddFixed(&a.force[5 * (size_t)a.stride + iatom], sz);
       }
     }
-    if (doVirial && !zeroShift) {
+    if (doVirial && doE64) {
+      // FP64 mode: the complete pair virial of this list, W = -sum g d (x) d
+      double tv[6], ts[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        tv[q] = warpSumD(wv[q]);
+        ts[q] = doSlow ? warpSumD(ws[q]) : 0.0;
+      }
+      if (lane < 18) {
+        const int q = symIndex(lane % 9);
+        double v = tv[0];
+#pragma unroll
+        for (int k = 1; k < 6; ++k)
+          if (k == q) v = (lane < 9) ? tv[k] : ts[k];
+        if (q == 0) v = (lane < 9) ? tv[0] : ts[0];
+        if (lane < 9 || doSlow) accVir += toFixedEnergy(v);
+      }
+    } else if (doVirial && !zeroShift) {
       // W[a][b] += (sum_i F_i)[a] * shift[b] for this list
       const long long Fx = warpSumLL((long long)qx), Fy = warpSumLL((long long)qy),
                       Fz = warpSumLL((long long)qz);
@@ -257,116 +313,83 @@ __global__ void __launch_bounds__(kForceThreads)
     if (doPairlist && lane == 0) a.listActive[L] = activeTiles;
   }  // lists
 
-  // block reduction of the fixed-point accumulators, then one atomic each
-  if (doEnergy || doVirial || doPairlist) {
-    long long* r = s_red[wib];
-    if (lane < kAccCount) r[lane] = 0;
-    __syncwarp();
-    if (doVirial && lane < 18) r[kAccVir + lane] = accVir;
-    if (doEnergy && lane == 0) {
-      r[kAccEVdw] = accE0;
-      r[kAccEElec] = accE1;
-      r[kAccESlow] = accE2;
-    }
-    if (doPairlist) {
-      int s = nexcl;
+  // per-warp flush of the fixed-point accumulators (no block barrier, so a
+  // warp that runs out of lists retires at once)
+  if (doVirial && lane < 18 && accVir != 0)
+    atomicAddFixed(&a.acc[kAccVir + lane], (unsigned long long)accVir);
+  if (doEnergy && lane == 0) {
+    if (accE0) atomicAddFixed(&a.acc[kAccEVdw], (unsigned long long)accE0);
+    if (accE1) atomicAddFixed(&a.acc[kAccEElec], (unsigned long long)accE1);
+    if (accE2) atomicAddFixed(&a.acc[kAccESlow], (unsigned long long)accE2);
+  }
+  if (doPairlist) {
+    int s = nexcl;
 #pragma unroll
-      for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) r[kAccNumExcl] = s;
-    }
-    if (doEnergy) {
-      int s = npair;
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0 && s) atomicAddFixed(&a.acc[kAccNumExcl], (unsigned long long)s);
+  }
+  if (doEnergy) {
+    int s = npair;
 #pragma unroll
-      for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) r[kAccNumPairs] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x < kAccCount) {
-      long long tot = 0;
-      for (int w = 0; w < kForceWarps; ++w) tot += s_red[w][threadIdx.x];
-      if (tot != 0) atomicAddFixed(&a.acc[threadIdx.x], (unsigned long long)tot);
-    }
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0 && s) atomicAddFixed(&a.acc[kAccNumPairs], (unsigned long long)s);
   }
 }
 
-template <bool E, bool V, bool S, bool P>
-static cudaError_t launchT(const ForceArgs& a, int grid, cudaStream_t st) {
+template <bool E, bool V, bool S, bool P, bool D>
+static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
   const size_t shmem = sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
-  auto k = forceKernel<E, V, S, P>;
-  if (shmem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+  auto k = forceKernel<E, V, S, P, D>;
+  static int cachedDim = -1, cachedBlocks = 0;
+  if (cachedDim != a.c.ljDim) {
+    if (shmem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+      if (e != cudaSuccess) return e;
+    }
+    int nb = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kForceThreads, shmem);
     if (e != cudaSuccess) return e;
+    cachedBlocks = nb > 0 ? nb : 1;
+    cachedDim = a.c.ljDim;
   }
-  k<<<grid, kForceThreads, shmem, st>>>(a);
+  k<<<numSM * cachedBlocks, kForceThreads, shmem, st>>>(a);
   return cudaGetLastError();
 }
 
-template <bool E, bool V, bool S, bool P>
-static int occupancyT(int ljDim) {
-  int nb = 0;
-  const size_t shmem = sizeof(float2) * (size_t)ljDim * ljDim;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, forceKernel<E, V, S, P>, kForceThreads, shmem);
-  return nb;
-}
-
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st) {
-  const bool E = flags & NBK_ENERGY, V = flags & NBK_VIRIAL, S = flags & NBK_SLOW,
-             P = flags & NBK_PAIRLIST;
-  const int idx = (E ? 8 : 0) | (V ? 4 : 0) | (S ? 2 : 0) | (P ? 1 : 0);
-  static int occ[16] = {0};
-  static int occDim[16] = {0};
-  int nb = (occDim[idx] == a.c.ljDim) ? occ[idx] : 0;
-  if (nb == 0) {
-#define NBK_OCC(i, e, v, s, p) \
-  case i:                      \
-    nb = occupancyT<e, v, s, p>(a.c.ljDim); \
-    break;
-    switch (idx) {
-      NBK_OCC(0, false, false, false, false)
-      NBK_OCC(1, false, false, false, true)
-      NBK_OCC(2, false, false, true, false)
-      NBK_OCC(3, false, false, true, true)
-      NBK_OCC(4, false, true, false, false)
-      NBK_OCC(5, false, true, false, true)
-      NBK_OCC(6, false, true, true, false)
-      NBK_OCC(7, false, true, true, true)
-      NBK_OCC(8, true, false, false, false)
-      NBK_OCC(9, true, false, false, true)
-      NBK_OCC(10, true, false, true, false)
-      NBK_OCC(11, true, false, true, true)
-      NBK_OCC(12, true, true, false, false)
-      NBK_OCC(13, true, true, false, true)
-      NBK_OCC(14, true, true, true, false)
-      NBK_OCC(15, true, true, true, true)
-    }
-#undef NBK_OCC
-    if (nb <= 0) nb = 1;
-    occ[idx] = nb;
-    occDim[idx] = a.c.ljDim;
-  }
-  const int grid = numSM * nb;
-#define NBK_LAUNCH(i, e, v, s, p) \
-  case i:                         \
-    return launchT<e, v, s, p>(a, grid, st);
+  const bool E = flags & NBK_ENERGY;
+  const int idx = (E ? 16 : 0) | ((flags & NBK_VIRIAL) ? 8 : 0) | ((flags & NBK_SLOW) ? 4 : 0) |
+                  ((flags & NBK_PAIRLIST) ? 2 : 0) | ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
   switch (idx) {
-    NBK_LAUNCH(0, false, false, false, false)
-    NBK_LAUNCH(1, false, false, false, true)
-    NBK_LAUNCH(2, false, false, true, false)
-    NBK_LAUNCH(3, false, false, true, true)
-    NBK_LAUNCH(4, false, true, false, false)
-    NBK_LAUNCH(5, false, true, false, true)
-    NBK_LAUNCH(6, false, true, true, false)
-    NBK_LAUNCH(7, false, true, true, true)
-    NBK_LAUNCH(8, true, false, false, false)
-    NBK_LAUNCH(9, true, false, false, true)
-    NBK_LAUNCH(10, true, false, true, false)
-    NBK_LAUNCH(11, true, false, true, true)
-    NBK_LAUNCH(12, true, true, false, false)
-    NBK_LAUNCH(13, true, true, false, true)
-    NBK_LAUNCH(14, true, true, true, false)
-    NBK_LAUNCH(15, true, true, true, true)
+#define NBK_CASE(i, e, v, s, p, d) \
+  case i:                          \
+    return launchT<e, v, s, p, d>(a, numSM, st);
+    NBK_CASE(0, false, false, false, false, false)
+    NBK_CASE(2, false, false, false, true, false)
+    NBK_CASE(4, false, false, true, false, false)
+    NBK_CASE(6, false, false, true, true, false)
+    NBK_CASE(8, false, true, false, false, false)
+    NBK_CASE(10, false, true, false, true, false)
+    NBK_CASE(12, false, true, true, false, false)
+    NBK_CASE(14, false, true, true, true, false)
+    NBK_CASE(16, true, false, false, false, false)
+    NBK_CASE(17, true, false, false, false, true)
+    NBK_CASE(18, true, false, false, true, false)
+    NBK_CASE(19, true, false, false, true, true)
+    NBK_CASE(20, true, false, true, false, false)
+    NBK_CASE(21, true, false, true, false, true)
+    NBK_CASE(22, true, false, true, true, false)
+    NBK_CASE(23, true, false, true, true, true)
+    NBK_CASE(24, true, true, false, false, false)
+    NBK_CASE(25, true, true, false, false, true)
+    NBK_CASE(26, true, true, false, true, false)
+    NBK_CASE(27, true, true, false, true, true)
+    NBK_CASE(28, true, true, true, false, false)
+    NBK_CASE(29, true, true, true, false, true)
+    NBK_CASE(30, true, true, true, true, false)
+    NBK_CASE(31, true, true, true, true, true)
+#undef NBK_CASE
   }
-#undef NBK_LAUNCH
   return cudaErrorInvalidValue;
 }
 

@@ -45,6 +45,14 @@ struct NbkConst {
   float one14;        // 1 - scale14
   int ljDim;          // LJ table row length
   int switching;      // 0 when switchdist >= cutoff (plain truncated LJ)
+  double hAd, hBd;    // hA, hB in FP64 (FP64 energy mode)
+  double betad;       // Ewald coefficient in FP64
+};
+
+// FP64 copies of the pair-math constants (FP64 energy/virial mode).
+struct NbkConst64 {
+  double rc2, rs2, lj0, lj1, lj2, lj3, rc3inv, hA, hB, beta, beta2Pi, one14;
+  int switching;
 };
 
 // Bounding box of one 32-atom tile: centre and half-widths.
@@ -81,6 +89,24 @@ __device__ __forceinline__ float3 shiftOf(const float3 o, const float3 a, const 
 // left to right (src/CudaComputeNonbondedKernel.cu:1225-1230).
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
   return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// erfc(x) = t P(t) exp(-x^2), t = 1/(1 + p x): Hastings' rational form (the
+// form of Abramowitz & Stegun 7.1.26) with a degree-7 P whose coefficients
+// were fitted by least squares on [0, 4] (fit_erfc.py; max relative error
+// 1.6e-8). `ex` is exp(-x^2), shared with the force's Gaussian term.
+constexpr float kErfcP = 4.067848869e-01f;
+__device__ __forceinline__ float erfcShared(const float x, const float ex) {
+  const float t = __fdividef(1.0f, fmaf(kErfcP, x, 1.0f));
+  float q = 8.043135869e-02f;
+  q = fmaf(q, t, -4.030445941e-01f);
+  q = fmaf(q, t, 6.621032108e-01f);
+  q = fmaf(q, t, -3.509793830e-01f);
+  q = fmaf(q, t, 3.971568035e-01f);
+  q = fmaf(q, t, 1.455091497e-01f);
+  q = fmaf(q, t, 2.400594718e-01f);
+  q = fmaf(q, t, 2.287639988e-01f);
+  return t * q * ex;
 }
 
 // FP32 pair math. f = (dE/dr)/r of LJ + fast electrostatics; fs = (dE/dr)/r
@@ -123,7 +149,7 @@ __device__ __forceinline__ void pairForce(const float r2, const float qq, const 
     const float r = r2 * rinv;
     const float x = c.beta * r;
     const float ex = __expf(-x * x);
-    const float ec = erfcf(x);
+    const float ec = erfcShared(x, ex);
     // slow (dE/dr)/r = qq ((1 - erfc - 2b/sqrt(pi) r e^{-x^2}) r^-3 - rc^-3)
     const float corr = fmaf(c.beta2Pi * r, ex, ec);
     fs = qq * fmaf(1.0f - corr, rinv3, -c.rc3inv);
@@ -131,6 +157,46 @@ __device__ __forceinline__ void pairForce(const float r2, const float qq, const 
   } else {
     fs = 0.0f;
   }
+}
+
+// The same pair math in FP64 from FP64 geometry d = x_j - x_i (FP64 energy
+// mode): g, gs = (dE/dr)/r of LJ + fast and of slow electrostatics; adds the
+// electrostatic energies to eE, eS.
+template <bool doSlow>
+__device__ __forceinline__ void pairFP64(const double r2, const double qq, const double A,
+                                         const double B, const NbkConst64& k, double& g,
+                                         double& gs, double& eE, double& eS) {
+  const double ri = rsqrt(r2);
+  const double ri2 = ri * ri, ri6 = ri2 * ri2 * ri2, ri3 = ri * ri2;
+  const double ab6 = fma(A, ri6, -B);
+  const double w = ab6 * ri6;
+  const double dw = fma(A, ri6, ab6) * (-6.0 * ri2 * ri6);
+  double s = 1.0, ds = 0.0;
+  if (k.switching) {
+    const double t2 = fmax(r2, k.rs2);
+    const double d = k.rc2 - t2;
+    s = d * d * fma(k.lj1, t2, k.lj0);
+    ds = d * fma(k.lj2, t2, k.lj3);
+  }
+  g = fma(w, ds, dw * s) + qq * (k.rc3inv - ri3);
+  const double h = fma(k.hB, r2, k.hA);
+  eE = fma(qq, ri - h, eE);
+  if (doSlow) {
+    const double r = r2 * ri, x = k.beta * r;
+    const double ec = erfc(x), ex = exp(-x * x);
+    gs = qq * fma(1.0 - ec - k.beta2Pi * r * ex, ri3, -k.rc3inv);
+    eS = fma(qq, fma(ec - 1.0, ri, h), eS);
+  } else {
+    gs = 0.0;
+  }
+}
+
+// Component k (0..8, row-major 3x3) of a symmetric tensor stored as
+// xx, xy, xz, yy, yz, zz.
+__device__ __forceinline__ int symIndex(int k) {
+  const int a = k / 3, b = k % 3;
+  const int lo = a < b ? a : b, hi = a < b ? b : a;
+  return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
 }
 
 __device__ __forceinline__ unsigned long long toFixedForce(float v) {
@@ -179,6 +245,8 @@ struct ForceArgs {
   long long* force;            // SoA [6][stride] fixed point
   int stride;
   long long* acc;              // [kAccCount]
+  int* workCounter;            // next list to hand out (zeroed before the launch)
+  NbkConst64 c64;              // FP64 energy/virial mode
 };
 
 }  // namespace nbk

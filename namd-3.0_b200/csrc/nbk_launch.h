@@ -34,6 +34,7 @@ struct CorrArgs {
   long long* force;
   int stride;
   long long* acc;
+  NbkConst64 c64;
 };
 cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st);
 

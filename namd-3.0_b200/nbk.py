@@ -106,6 +106,7 @@ class PackedView(C.Structure):
 
 
 NBK_ENERGY, NBK_VIRIAL, NBK_SLOW, NBK_PAIRLIST, NBK_CORRECTIONS = 1, 2, 4, 8, 16
+NBK_ENERGY_FP64 = 32
 NBK_SYS_WATER, NBK_SYS_MIXED = 0, 1
 FORCE_FIXED_SCALE = float(2 ** 32)   # fixed-point units per kcal/mol/A
 

@@ -4,8 +4,8 @@ import pytest
 
 import nbk
 import oracle
-from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, PARAMS, VIRIAL_TOL, GpuRun, compare,
-                     mixed_box, real_slots, water_box)
+from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, FP32_ELEC_ENERGY_TOL, PARAMS, VIRIAL_TOL,
+                     GpuRun, compare, mixed_box, real_slots, water_box)
 
 pytestmark = pytest.mark.gpu
 
@@ -46,42 +46,48 @@ def test_pairset_mixed(mixed):
     _pairset_check(mixed[1], mixed[2])
 
 
-@pytest.mark.parametrize("corr", [False, True])
-def test_forces_water(water, corr):
-    s, p, o = water
+def _check_forces(system, corr, e64):
+    s, p, o = system
     mode = 3 if corr else 1
-    extra = nbk.NBK_CORRECTIONS if corr else 0
+    extra = (nbk.NBK_CORRECTIONS if corr else 0) | (nbk.NBK_ENERGY_FP64 if e64 else 0)
     Fo, So, ro = o.forces(mode)
     run = GpuRun(p)
     run.build()
     real = real_slots(p)
+    etol = ENERGY_TOL if e64 else FP32_ELEC_ENERGY_TOL
     for flags in (ALL | nbk.NBK_PAIRLIST | extra, ALL | extra):
         F, S, res, _ = run.eval(flags)
         err = compare(F, S, res, Fo, So, ro, real)
-        print(flags, err)
-        assert err["force"] <= FORCE_RMS_TOL and err["slow"] <= FORCE_RMS_TOL
-        for k in ("energyVdw", "energyElec", "energySlow"):
-            assert err[k] <= ENERGY_TOL, (k, err)
+        print(f"flags={flags} " + " ".join(f"{k}={v:.2e}" for k, v in err.items()))
+        assert err["force"] <= FORCE_RMS_TOL and err["slow"] <= FORCE_RMS_TOL, err
+        assert err["energyVdw"] <= ENERGY_TOL, err
+        assert err["energyElec"] <= etol and err["energySlow"] <= etol, err
         assert err["virial"] <= VIRIAL_TOL and err["virialSlow"] <= VIRIAL_TOL, err
 
 
 @pytest.mark.parametrize("corr", [False, True])
-def test_forces_mixed(mixed, corr):
+@pytest.mark.parametrize("e64", [False, True])
+def test_forces_water(water, corr, e64):
+    _check_forces(water, corr, e64)
+
+
+@pytest.mark.parametrize("corr", [False, True])
+@pytest.mark.parametrize("e64", [False, True])
+def test_forces_mixed(mixed, corr, e64):
+    _check_forces(mixed, corr, e64)
+
+
+def test_pair_count(mixed):
+    """The GPU's count of interacting pairs (the benchmark's work unit)
+    equals the oracle's."""
     s, p, o = mixed
-    mode = 3 if corr else 1
-    extra = nbk.NBK_CORRECTIONS if corr else 0
-    Fo, So, ro = o.forces(mode)
+    _, _, ro = o.forces(1)
     run = GpuRun(p)
     run.build()
-    real = real_slots(p)
-    for flags in (ALL | nbk.NBK_PAIRLIST | extra, ALL | extra):
-        F, S, res, _ = run.eval(flags)
-        err = compare(F, S, res, Fo, So, ro, real)
-        print(flags, err)
-        assert err["force"] <= FORCE_RMS_TOL and err["slow"] <= FORCE_RMS_TOL
-        for k in ("energyVdw", "energyElec", "energySlow"):
-            assert err[k] <= ENERGY_TOL, (k, err)
-        assert err["virial"] <= VIRIAL_TOL and err["virialSlow"] <= VIRIAL_TOL, err
+    run.eval(ALL | nbk.NBK_PAIRLIST)
+    assert run.nb.pair_count() == ro["pairs"]
+    run.eval(ALL)
+    assert run.nb.pair_count() == ro["pairs"]
 
 
 def test_deterministic(mixed):
