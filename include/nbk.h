@@ -226,6 +226,37 @@ NBK_API int nbk_export_tile_lists(nbk_handle h, int* numTileLists, int* numJtile
                                   nbk_tile_list* tileLists, int* tileJatomStart,
                                   nbk_tile_excl* tileExcls, void* stream);
 
+/* ---- allocation-free variant ------------------------------------------------ */
+
+/* No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (a host framework that owns all device memory through its own pool, code
+ * between captured regions that must not touch the allocator, runtimes with a
+ * device heap fixed at start-up): the excluded / modified (1-4) pair
+ * corrections of NBK_CORRECTIONS without a handle and without allocating.
+ * Scratch (fixed-point accumulators and a tuple staging copy) is a static
+ * device array of about 11 MB that every GPU loading the library holds until
+ * exit; it limits atomStorageSize to 65,536 slots and numModified + numExcluded
+ * to 262,144 tuples (larger sizes return NBK_ERR_ARG). Inputs: device xyzq,
+ * device LJ delta table float2[ljDim*ljDim] = (A14 - A, B14 - B) * scaling,
+ * host tuple arrays (validated, then copied into the scratch); scalar fields of
+ * params (cutoff, switchdist, ewaldcof, scale14) are read, its LJ arrays are
+ * not. flags: NBK_ENERGY | NBK_VIRIAL | NBK_SLOW (and NBK_ENERGY_FP64 is not
+ * accepted). Outputs: device float4 forces (and slow forces with NBK_SLOW),
+ * device nbk_virial_energy with NBK_ENERGY or NBK_VIRIAL. The first call on a
+ * device looks up the scratch address for that device; make it before any
+ * stream capture. All calls share the scratch: calls that overlap on the GPU
+ * race, so the caller serialises them (same stream, one at a time). */
+NBK_API int nbk_exclusion_force_noalloc(const nbk_params* params, const float* d_ljExclTable,
+                                        int ljDim, int atomStorageSize, const nbk_float4* d_xyzq,
+                                        int numModified, const nbk_exclusion* h_modified,
+                                        int numExcluded, const nbk_exclusion* h_excluded,
+                                        nbk_float3 lata, nbk_float3 latb, nbk_float3 latc,
+                                        unsigned flags, nbk_float4* d_forces,
+                                        nbk_float4* d_forcesSlow, nbk_virial_energy* d_ve,
+                                        void* stream);
+/* Message of the last failure of nbk_exclusion_force_noalloc on this thread. */
+NBK_API const char* nbk_noalloc_last_error(void);
+
 /* ---- measurement ----------------------------------------------------------- */
 
 /* Enables (1) or disables (0) CUDA-event timing of every force-kernel launch
