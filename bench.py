@@ -344,6 +344,167 @@ def run_gpu(args, rank, world, local_rank):
     nb.close()
 
 
+BATCH_METRIC = ("replica-evals/s, 64 replicas of 2,000-40,000 atoms in one launch (CUDA graph) "
+                "vs one launch per replica")
+
+
+def run_batch(args, rank, world, local_rank):
+    """64 independent replicas (log-uniform 2k-40k atoms, 0.1 atoms/A^3, own
+    seeds): the batched handle's steady-state evaluation captured in a CUDA
+    graph, against the same replicas evaluated one handle and one launch each."""
+    import torch
+    import nbk
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(20261203 + rank)
+    sizes = np.exp(rng.uniform(np.log(2000), np.log(40000), 64)).astype(int)
+    systems = [nbk.System(nbk.NBK_SYS_MIXED, 5000 + 100 * rank + r, int(n), FRAC)
+               for r, n in enumerate(sizes)]
+    many = nbk.Packed.many(systems)
+    params = nbk.NonbondedParams()
+    FL = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
+    stream = torch.cuda.Stream(dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        st = stream.cuda_stream
+        nb = nbk.Nonbonded(params, systems[0].lj_table(), local_rank)
+        nb.setup(many, stream=st)
+        nb.set_replicas(many, stream=st)
+        x = torch.from_numpy(many.xyzq.copy()).to(dev)
+        n = many.atomStorageSize
+        dF = torch.zeros((n, 4), device=dev)
+        dS = torch.zeros((n, 4), device=dev)
+        dVE = torch.zeros((64, 32), dtype=torch.float64, device=dev)
+        nb.build_tile_lists(many, xyzq=x, stream=st)
+        nb.force(many, FL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+        nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+        pairs = int(nb.pair_counts(st).sum())
+        for _ in range(args.warmup):
+            nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+            nb.virial_energy_batch_to(dVE.data_ptr(), True, stream=st)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            cs = torch.cuda.current_stream().cuda_stream
+            nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=cs)
+            nb.virial_energy_batch_to(dVE.data_ptr(), True, stream=cs)
+        for _ in range(3):
+            g.replay()
+        stream.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            g.replay()
+            ev[k][1].record(stream)
+        stream.synchronize()
+        batched_ms = sum(a.elapsed_time(b) for a, b in ev)
+
+        # plain path: one handle per replica, one launch sequence per replica
+        plain = []
+        for r, sy in enumerate(systems):
+            pk = nbk.Packed(sy)
+            h = nbk.Nonbonded(params, sy.lj_table(), local_rank)
+            h.setup(pk, stream=st)
+            xr = torch.from_numpy(pk.xyzq.copy()).to(dev)
+            fr = torch.zeros((pk.atomStorageSize, 4), device=dev)
+            sr = torch.zeros((pk.atomStorageSize, 4), device=dev)
+            ver = torch.zeros(32, dtype=torch.float64, device=dev)
+            h.build_tile_lists(pk, xyzq=xr, stream=st)
+            h.force(pk, FL | nbk.NBK_PAIRLIST, xyzq=xr, d_forces=fr, d_forcesSlow=sr, stream=st)
+            plain.append((h, pk, xr, fr, sr, ver))
+        ksteps = max(3, min(args.steps, 200))
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(ksteps)]
+        for k in range(args.warmup + ksteps):
+            if k >= args.warmup:
+                flush.zero_()
+                pev[k - args.warmup][0].record(stream)
+            for h, pk, xr, fr, sr, ver in plain:
+                h.force(pk, FL, xyzq=xr, d_forces=fr, d_forcesSlow=sr, stream=st)
+                h.virial_energy_to(ver.data_ptr(), True, stream=st)
+            if k >= args.warmup:
+                pev[k - args.warmup][1].record(stream)
+        stream.synchronize()
+        plain_ms = sum(a.elapsed_time(b) for a, b in pev)
+    batched = 64 * args.steps / (batched_ms * 1e-3)
+    plainv = 64 * ksteps / (plain_ms * 1e-3)
+    print(json.dumps({
+        "metric": BATCH_METRIC, "value": batched, "unit": "replica-evals/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "batch64: 64 mixed replicas, log-uniform 2,000-40,000 atoms, "
+                               "0.1 atoms/A^3, own seeds; steady-state force+energy+virial+slow",
+                   "atoms": int(sizes.sum()), "pairs_per_batch_eval": pairs,
+                   "l2": "flushed between timed steps"},
+        "pairs_per_s": pairs * args.steps / (batched_ms * 1e-3),
+        "plain_one_launch_per_replica": {"value": plainv, "unit": "replica-evals/s",
+                                         "ms_per_step": plain_ms / ksteps, "steps": ksteps},
+        "speedup_vs_plain": batched / plainv,
+    }))
+
+
+def run_adjoint(args, rank, world, local_rank):
+    """24,000-atom mixed system: the adjoint (gradient of sum w.F + 0.1 E for
+    positions, charges and LJ parameters, recomputed from the tile lists)
+    against one forward force+energy+virial evaluation of the same lists."""
+    import torch
+    import nbk
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    sy = nbk.System(nbk.NBK_SYS_MIXED, 77 + rank, 24000, FRAC)
+    p = nbk.Packed(sy)
+    n = p.atomStorageSize
+    dim = sy.lj_table()[0]
+    nb = nbk.Nonbonded(nbk.NonbondedParams(), sy.lj_table(), local_rank)
+    stream = torch.cuda.current_stream(dev)
+    st = stream.cuda_stream
+    nb.setup(p, stream=st)
+    x = torch.from_numpy(p.xyzq.copy()).to(dev)
+    rng = np.random.default_rng(24)
+    w = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    w[:, :3] = torch.from_numpy(rng.standard_normal((n, 3)).astype(np.float32)).to(dev)
+    g = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    gab = torch.zeros(2 * dim * dim, dtype=torch.float64, device=dev)
+    mask = np.zeros(dim, dtype=np.int32)
+    mask[:dim - 2] = 1
+    FL = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
+    dF = torch.zeros((n, 4), device=dev)
+    dS = torch.zeros((n, 4), device=dev)
+    nb.build_tile_lists(p, xyzq=x, stream=st)
+    nb.force(p, FL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+    for _ in range(args.warmup):
+        nb.force(p, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+        nb.adjoint(w, w, 0.1, 0.1, 0.1, g, gab, type_mask=mask, stream=st)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    ev_f = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.steps)]
+    ev_a = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        ev_f[k][0].record(stream)
+        nb.force(p, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
+        ev_f[k][1].record(stream)
+        flush.zero_()
+        ev_a[k][0].record(stream)
+        nb.adjoint(w, w, 0.1, 0.1, 0.1, g, gab, type_mask=mask, stream=st)
+        ev_a[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    fwd = sum(a.elapsed_time(b) for a, b in ev_f) / args.steps
+    adj = sum(a.elapsed_time(b) for a, b in ev_a) / args.steps
+    print(json.dumps({
+        "metric": "adjoint cost / forward cost, 24,000 atoms", "value": adj / fwd, "unit": "ratio",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+        "data": "synthetic", "dtype": "f32",
+        "config": {"workload": "adjoint24k: 24,000-atom mixed system, L = sum w.(F+Fslow) + "
+                               "0.1 (E_vdw+E_elec+E_slow), gradients for positions, charges and "
+                               "the 32 solute types' LJ parameters"},
+        "forward_ms": fwd, "adjoint_ms": adj}))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -352,6 +513,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--workload", choices=["mixed92k", "batch64", "adjoint24k"], default="mixed92k",
+                    help="batch64: 64-replica batched launch vs one launch per replica")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -360,6 +523,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "batch64":
+        run_batch(args, rank, world, local_rank)
+        return
+    if args.workload == "adjoint24k":
+        run_adjoint(args, rank, world, local_rank)
         return
     if world > 1:
         import datetime

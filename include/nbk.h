@@ -226,6 +226,50 @@ NBK_API int nbk_export_tile_lists(nbk_handle h, int* numTileLists, int* numJtile
                                   nbk_tile_list* tileLists, int* tileJatomStart,
                                   nbk_tile_excl* tileExcls, void* stream);
 
+/* ---- adjoint ------------------------------------------------------------------- */
+
+/* No counterpart in the reference. Gradient of
+ *   L = sum_i wF_i.F_i + sum_i wS_i.Fslow_i + cV E_vdw + cE E_elec + cS E_slow
+ * for the last refined tile lists and the bound positions (call after an
+ * nbk_nonbonded_force of the same positions): with respect to the positions
+ * (a Hessian-vector product), the scaled charges xyzq.w, and the scaled LJ
+ * table entries. Pair terms are recomputed from the tile lists; nothing of
+ * the forward pass is stored. wS and cS are used with NBK_SLOW in flags.
+ *   d_wF, d_wS   : device float4[atomStorageSize] cotangents (w ignored)
+ *   h_typeMask   : host int[vdwTableDim]; LJ gradients are accumulated for
+ *                  pairs that touch a type with a non-zero entry (NULL: all)
+ *   d_gradXQ     : device float4[atomStorageSize] (dL/dx, dL/dy, dL/dz, dL/dq)
+ *   d_gradFixed  : optional device int64[4*atomStorageSize] SoA, 2^32 units
+ *   d_gradAB     : device double[2*dim*dim]: dL/dA then dL/dB at ordered type
+ *                  pairs (i-type, j-type); fold with nbk_lj_param_grad */
+NBK_API int nbk_adjoint(nbk_handle h, unsigned flags, const nbk_float4* d_wF,
+                        const nbk_float4* d_wS, double cV, double cE, double cS,
+                        const int* h_typeMask, nbk_float4* d_gradXQ, long long* d_gradFixed,
+                        double* d_gradAB, void* stream);
+
+/* ---- batched replicas -------------------------------------------------------- */
+
+/* No counterpart in the reference (NAMD runs independent systems as separate
+ * processes). Turns the handle into a batch of numReplicas independent
+ * systems evaluated by the same launches: the computes, patches and atom slots
+ * given to the other calls are the replicas' arrays concatenated (replica r
+ * owns atom slots [replicaSlotStart[r], replicaSlotStart[r+1]) and the computes
+ * with replicaOfCompute[c] == r), each replica with its own lattice (a, b, c)
+ * and its own LJ tables ljA/ljB/ljA14/ljB14 [numReplicas][dim*dim] (dim =
+ * params.vdwTableDim). Call after nbk_update_computes; the lattice arguments
+ * of later calls are then ignored. Energies, virials and pair counts are kept
+ * per replica (nbk_reduce_virial_energy_batch, nbk_get_pair_counts).
+ * NBK_ENERGY_FP64 is not available in batched mode. */
+NBK_API int nbk_set_replicas(nbk_handle h, int numReplicas, const int* h_replicaOfCompute,
+                             const int* h_replicaSlotStart, const nbk_float3* h_lattices,
+                             const double* ljA, const double* ljB, const double* ljA14,
+                             const double* ljB14, void* stream);
+/* Per-replica VirialEnergy records of the last evaluation: ve[numReplicas]. */
+NBK_API int nbk_reduce_virial_energy_batch(nbk_handle h, unsigned flags, nbk_virial_energy* ve,
+                                           int veOnDevice, void* stream);
+/* Per-replica pair counts of the last NBK_ENERGY evaluation (synchronises). */
+NBK_API int nbk_get_pair_counts(nbk_handle h, long long* counts, int maxCount, void* stream);
+
 /* ---- allocation-free variant ------------------------------------------------ */
 
 /* No counterpart in the reference. For callers that cannot call cudaMalloc

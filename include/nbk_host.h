@@ -76,6 +76,14 @@ NBK_API int nbk_system_free(nbk_system s);
 NBK_API int nbk_lj_table(int ntypes, const double* sigma, const double* epsilon,
                          int geometric, double* A, double* B, double* A14, double* B14);
 
+/* Chain rule of the adjoint's LJ output: gradients w.r.t. the scaled table
+ * entries (gA, gB at ordered type pair [i*ntypes + j]) to per-type sigma and
+ * epsilon under the combining rule of nbk_lj_table. Types with epsilon 0
+ * receive no epsilon gradient (the combining rule is not differentiable there). */
+NBK_API int nbk_lj_param_grad(int ntypes, const double* sigma, const double* epsilon, int geometric,
+                              double scaling, const double* gA, const double* gB, double* gSigma,
+                              double* gEps);
+
 /* ---- packing (host mirror of CudaComputeNonbonded's input preparation) ---- */
 typedef struct nbk_packed_s* nbk_packed;
 
@@ -101,12 +109,23 @@ typedef struct {
   nbk_exclusion* excluded;          /* [numExcluded] full-exclusion tuples */
   int* slotOfAtom;                  /* [natoms] global atom -> slot */
   double* patchCenter;              /* [3*numPatches] unscaled centres (A) */
+  /* replicas (nbk_pack_many; a single packing is one replica) */
+  int numReplicas;
+  int* replicaOfCompute;            /* [numComputes] */
+  int* replicaSlotStart;            /* [numReplicas+1] slot range of each replica */
+  int* replicaAtomStart;            /* [numReplicas+1] atom range (global ids) */
+  nbk_float3* replicaLattice;       /* [3*numReplicas] a, b, c of each replica */
 } nbk_packed_view;
 
 /* patchDim: patch side lower bound (NAMD: pairlistdist, src/SimParameters.C:3481).
  * coulombScaling = scaling / dielectric; q = charge*sqrt(332.0636*coulombScaling). */
 NBK_API int nbk_pack(nbk_system s, double patchDim, double coulombScaling, nbk_packed* out);
 NBK_API int nbk_packed_view_get(nbk_packed p, nbk_packed_view* v);
+/* Packs n independent systems (replicas) into one concatenated layout: patch,
+ * compute, slot and atom indices and exclusion-bit bases are offset per replica
+ * so that one handle evaluates all of them (nbk_set_replicas). */
+NBK_API int nbk_pack_many(const nbk_system* systems, int n, double patchDim,
+                          double coulombScaling, nbk_packed* out);
 /* Re-pack xyzq from the system's current positions, keeping the patch
  * assignment and slot order (steps between pairlist rebuilds). */
 NBK_API int nbk_pack_update_positions(nbk_packed p, nbk_system s);

@@ -111,6 +111,16 @@ struct nbk_context {
   int numMod = 0, numExc = 0;
   int maxTupleSlot = -1;  // largest atom slot named by a correction tuple
   unsigned lastFlags = 0;
+  // batched replicas (0 = single system)
+  int nrep = 0;
+  DBuf<int> compRep, slotRep;
+  DBuf<float3> repLat;
+  DBuf<float2> repLJ, repLJExcl;
+  int slotRepSize = 0;
+  // adjoint
+  DBuf<long long> adjGrad;
+  DBuf<int> typeMask;
+  int adjStride = 0;
   // measurement
   long long launches = 0;
   bool timing = false;
@@ -202,6 +212,7 @@ int bindPositions(nbk_handle h, const nbk_float4* xyzq, int onDevice, int n, cud
     return NBK_OK;
   }
   if (onDevice) {
+    if (reinterpret_cast<const float4*>(xyzq) == h->xyzq) return NBK_OK;  // already bound
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, xyzq) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
       cudaGetLastError();
@@ -312,6 +323,13 @@ NBK_API int nbk_destroy(nbk_handle h) {
   h->ve.release();
   h->modTuples.release();
   h->excTuples.release();
+  h->adjGrad.release();
+  h->typeMask.release();
+  h->compRep.release();
+  h->slotRep.release();
+  h->repLat.release();
+  h->repLJ.release();
+  h->repLJExcl.release();
   for (cudaEvent_t e : h->evStart) cudaEventDestroy(e);
   for (cudaEvent_t e : h->evStop) cudaEventDestroy(e);
   delete h;
@@ -484,8 +502,11 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
   // culling distance: the pairlist cutoff inflated by a relative 1e-5 so FP32
   // rounding in the boxes can never drop a pair the exact pair test keeps
   const float cull2 = plcutoff2 * 1.00002f + 1e-6f;
+  if (h->nrep > 0 && h->slotRepSize != atomStorageSize)
+    return setErr(NBK_ERR_STATE, "nbk_build_tile_lists: atomStorageSize differs from the replica layout");
   NBK_CUDA(launchBuildLists(h->numLists, h->seeds.p, h->computes.p, h->patches.p, h->bboxes.p,
-                            h->lata, h->latb, h->latc, cull2, h->lists1.p, h->patchPairs.p,
+                            h->lata, h->latb, h->latc, h->nrep ? h->compRep.p : nullptr,
+                            h->nrep ? h->repLat.p : nullptr, cull2, h->lists1.p, h->patchPairs.p,
                             h->jatom1.p, st), "tile-list build");
   h->c.plcutoff2 = plcutoff2;
   h->built = true;
@@ -519,7 +540,11 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     h->forceStride = n;
   }
   NBK_CUDA(cudaMemsetAsync(h->force.p, 0, sizeof(long long) * 6 * (size_t)n, st), "nbk_nonbonded_force");
-  NBK_CUDA(cudaMemsetAsync(h->acc.p, 0, sizeof(long long) * kAccCount, st), "nbk_nonbonded_force");
+  if (h->nrep > 0 && (flags & NBK_ENERGY_FP64) && (flags & NBK_ENERGY))
+    return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: NBK_ENERGY_FP64 is not available with replicas");
+  const int accBlocks = h->nrep > 0 ? h->nrep : 1;
+  NBK_CUDA(cudaMemsetAsync(h->acc.p, 0, sizeof(long long) * kAccCount * (size_t)accBlocks, st),
+           "nbk_nonbonded_force");
   h->lata = f3(lata);
   h->latb = f3(latb);
   h->latc = f3(latc);
@@ -542,6 +567,11 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   a.acc = h->acc.p;
   a.workCounter = h->counters.p + 2;
   a.c64 = h->c64;
+  if (h->nrep > 0) {
+    a.compRep = h->compRep.p;
+    a.repLat = h->repLat.p;
+    a.repLJ = h->repLJ.p;
+  }
   NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
   if (pairlist) {
     a.lists = h->lists1.p;
@@ -595,12 +625,18 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     ca.stride = n;
     ca.acc = h->acc.p;
     ca.c64 = h->c64;
+    if (h->nrep > 0) {
+      ca.slotRep = h->slotRep.p;
+      ca.repLat = h->repLat.p;
+      ca.repLJExcl = h->repLJExcl.p;
+    }
     NBK_CUDA(launchCorrections(ca, flags, st), "exclusion corrections");
     h->launches += 1;
   }
   NBK_CUDA(launchFinalizeForces(n, h->force.p, n, h->xyzq, reinterpret_cast<float4*>(d_forces),
                                 (flags & NBK_SLOW) ? reinterpret_cast<float4*>(d_forcesSlow) : nullptr,
-                                flags, h->acc.p, h->numSM, st), "force finalize");
+                                flags, h->acc.p, h->numSM, st, h->nrep ? h->slotRep.p : nullptr),
+           "force finalize");
   if ((flags & NBK_VIRIAL) || d_forces || d_forcesSlow) h->launches += 1;
   if (d_forcesFixed)
     NBK_CUDA(cudaMemcpyAsync(d_forcesFixed, h->force.p, sizeof(long long) * 6 * (size_t)n,
@@ -625,6 +661,8 @@ NBK_API int nbk_reduce_virial_energy(nbk_handle h, unsigned flags, nbk_virial_en
   if (rc) return rc;
   (void)flags;
   if (!ve) return setErr(NBK_ERR_ARG, "nbk_reduce_virial_energy: NULL output");
+  if (h->nrep > 0)
+    return setErr(NBK_ERR_STATE, "nbk_reduce_virial_energy: the handle holds replicas; use nbk_reduce_virial_energy_batch");
   cudaStream_t st = (cudaStream_t)stream;
   nbk_virial_energy* dst = veOnDevice ? ve : h->ve.p;
   NBK_CUDA(launchEnergyVirial(h->acc.p, dst, st), "energy/virial read-out");
@@ -641,10 +679,14 @@ NBK_API int nbk_get_tile_list_stat(nbk_handle h, nbk_tile_list_stat* out, void* 
   if (!out) return setErr(NBK_ERR_ARG, "nbk_get_tile_list_stat: NULL output");
   cudaStream_t st = (cudaStream_t)stream;
   int cnt[2] = {0, 0};
-  long long nex = 0;
+  const int accBlocks = h->nrep > 0 ? h->nrep : 1;
+  std::vector<long long> accHost((size_t)kAccCount * accBlocks);
   NBK_CUDA(cudaMemcpyAsync(cnt, h->counters.p, sizeof(int) * 2, cudaMemcpyDeviceToHost, st), "stat");
-  NBK_CUDA(cudaMemcpyAsync(&nex, h->acc.p + kAccNumExcl, sizeof(long long), cudaMemcpyDeviceToHost, st), "stat");
+  NBK_CUDA(cudaMemcpyAsync(accHost.data(), h->acc.p, sizeof(long long) * accHost.size(),
+                           cudaMemcpyDeviceToHost, st), "stat");
   NBK_CUDA(cudaStreamSynchronize(st), "stat");
+  long long nex = 0;
+  for (int r = 0; r < accBlocks; ++r) nex += accHost[(size_t)r * kAccCount + kAccNumExcl];
   std::memset(out, 0, sizeof(*out));
   out->numTileLists = h->refined ? cnt[0] : h->numLists;
   out->numTileListsGBIS = out->numTileLists;
@@ -671,6 +713,153 @@ NBK_API int nbk_export_tile_lists(nbk_handle h, int* numTileLists, int* numJtile
     NBK_CUDA(cudaMemcpy(jatom, h->jatom2.p, sizeof(int) * cnt[1], cudaMemcpyDeviceToHost), "export");
   if (excl && cnt[1])
     NBK_CUDA(cudaMemcpy(excl, h->excl2.p, sizeof(nbk_tile_excl) * cnt[1], cudaMemcpyDeviceToHost), "export");
+  return NBK_OK;
+}
+
+NBK_API int nbk_adjoint(nbk_handle h, unsigned flags, const nbk_float4* d_wF, const nbk_float4* d_wS,
+                        double cV, double cE, double cS, const int* h_typeMask,
+                        nbk_float4* d_gradXQ, long long* d_gradFixed, double* d_gradAB,
+                        void* stream) {
+  int rc = checkHandle(h, "nbk_adjoint");
+  if (rc) return rc;
+  if (!d_wF || !d_gradAB) return setErr(NBK_ERR_ARG, "nbk_adjoint: NULL argument");
+  if (flags & ~(unsigned)NBK_SLOW) return setErr(NBK_ERR_ARG, "nbk_adjoint: only NBK_SLOW applies");
+  const bool slow = flags & NBK_SLOW;
+  if (slow && !d_wS) return setErr(NBK_ERR_ARG, "nbk_adjoint: NBK_SLOW needs d_wS");
+  if (!h->refined || !h->xyzq)
+    return setErr(NBK_ERR_STATE, "nbk_adjoint: needs refined tile lists (an NBK_PAIRLIST evaluation) first");
+  if (h->nrep > 0) return setErr(NBK_ERR_STATE, "nbk_adjoint: not available with replicas");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = h->atomStorageSize, dim = h->ljDim;
+  std::vector<int> mask(dim, 1);
+  if (h_typeMask)
+    for (int t = 0; t < dim; ++t) mask[t] = h_typeMask[t] ? 1 : 0;
+  NBK_CUDA(h->typeMask.ensure(dim), "nbk_adjoint");
+  NBK_CUDA(cudaMemcpyAsync(h->typeMask.p, mask.data(), sizeof(int) * dim, cudaMemcpyHostToDevice, st),
+           "nbk_adjoint");
+  if (h->adjStride != n) {
+    NBK_CUDA(h->adjGrad.ensure(4 * (size_t)n), "nbk_adjoint");
+    h->adjStride = n;
+  }
+  NBK_CUDA(cudaMemsetAsync(h->adjGrad.p, 0, sizeof(long long) * 4 * (size_t)n, st), "nbk_adjoint");
+  NBK_CUDA(cudaMemsetAsync(d_gradAB, 0, sizeof(double) * 2 * (size_t)dim * dim, st), "nbk_adjoint");
+  NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_adjoint");
+  AdjArgs a{};
+  a.lists = h->lists2.p;
+  a.numListsDev = h->counters.p;
+  a.tileJatomStart = h->jatom2.p;
+  a.tileExcls = h->excl2.p;
+  a.xyzq = h->xyzq;
+  a.vdwTypes = h->vdwTypes.p;
+  a.ljTable = h->ljTable.p;
+  a.typeMask = h->typeMask.p;
+  a.wF = reinterpret_cast<const float4*>(d_wF);
+  a.wS = reinterpret_cast<const float4*>(d_wS);
+  a.cV = (float)cV;
+  a.cE = (float)cE;
+  a.cS = (float)cS;
+  a.lata = h->lata;
+  a.latb = h->latb;
+  a.latc = h->latc;
+  a.c = h->c;
+  a.grad = h->adjGrad.p;
+  a.stride = n;
+  a.gradAB = d_gradAB;
+  a.workCounter = h->counters.p + 2;
+  NBK_CUDA(timedEvent(h, true, st), "timing event");
+  NBK_CUDA(launchAdjoint(a, slow, h->numSM, n, reinterpret_cast<float4*>(d_gradXQ), st), "adjoint kernel");
+  NBK_CUDA(timedEvent(h, false, st), "timing event");
+  h->launches += d_gradXQ ? 2 : 1;
+  if (d_gradFixed)
+    NBK_CUDA(cudaMemcpyAsync(d_gradFixed, h->adjGrad.p, sizeof(long long) * 4 * (size_t)n,
+                             cudaMemcpyDeviceToDevice, st), "nbk_adjoint: fixed-point copy");
+  return NBK_OK;
+}
+
+NBK_API int nbk_set_replicas(nbk_handle h, int numReplicas, const int* repOfCompute,
+                             const int* slotStart, const nbk_float3* lattices, const double* ljA,
+                             const double* ljB, const double* ljA14, const double* ljB14,
+                             void* stream) {
+  int rc = checkHandle(h, "nbk_set_replicas");
+  if (rc) return rc;
+  if (numReplicas <= 0 || !repOfCompute || !slotStart || !lattices || !ljA || !ljB)
+    return setErr(NBK_ERR_ARG, "nbk_set_replicas: bad argument");
+  if (!h->numComputes) return setErr(NBK_ERR_STATE, "nbk_set_replicas: call nbk_update_computes first");
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int c = 0; c < h->numComputes; ++c)
+    if (repOfCompute[c] < 0 || repOfCompute[c] >= numReplicas)
+      return setErr(NBK_ERR_ARG, "nbk_set_replicas: replica index of a compute out of range");
+  if (slotStart[0] != 0) return setErr(NBK_ERR_ARG, "nbk_set_replicas: replicaSlotStart[0] must be 0");
+  for (int r = 0; r < numReplicas; ++r)
+    if (slotStart[r + 1] < slotStart[r] || (slotStart[r] & 31))
+      return setErr(NBK_ERR_ARG, "nbk_set_replicas: replica slot ranges must increase in multiples of 32");
+  const int n = slotStart[numReplicas];
+  std::vector<int> slotRep(n);
+  for (int r = 0; r < numReplicas; ++r)
+    for (int k = slotStart[r]; k < slotStart[r + 1]; ++k) slotRep[k] = r;
+  const int dim = h->ljDim, d2 = dim * dim;
+  std::vector<float2> t((size_t)numReplicas * d2), te((size_t)numReplicas * d2);
+  const double sc = h->prm.scaling;
+  for (size_t k = 0; k < t.size(); ++k) {
+    t[k] = make_float2((float)(ljA[k] * sc), (float)(ljB[k] * sc));
+    const double a14 = ljA14 ? ljA14[k] : ljA[k], b14 = ljB14 ? ljB14[k] : ljB[k];
+    te[k] = make_float2((float)((a14 - ljA[k]) * sc), (float)((b14 - ljB[k]) * sc));
+  }
+  NBK_CUDA(h->compRep.ensure(h->numComputes), "nbk_set_replicas");
+  NBK_CUDA(h->slotRep.ensure(std::max(n, 1)), "nbk_set_replicas");
+  NBK_CUDA(h->repLat.ensure(3 * (size_t)numReplicas), "nbk_set_replicas");
+  NBK_CUDA(h->repLJ.ensure(t.size()), "nbk_set_replicas");
+  NBK_CUDA(h->repLJExcl.ensure(te.size()), "nbk_set_replicas");
+  NBK_CUDA(h->acc.ensure((size_t)kAccCount * numReplicas), "nbk_set_replicas");
+  NBK_CUDA(h->ve.ensure(numReplicas), "nbk_set_replicas");
+  NBK_CUDA(cudaMemcpy(h->compRep.p, repOfCompute, sizeof(int) * h->numComputes, cudaMemcpyHostToDevice),
+           "nbk_set_replicas");
+  if (n) NBK_CUDA(cudaMemcpy(h->slotRep.p, slotRep.data(), sizeof(int) * n, cudaMemcpyHostToDevice), "nbk_set_replicas");
+  NBK_CUDA(cudaMemcpy(h->repLat.p, lattices, sizeof(float3) * 3 * (size_t)numReplicas, cudaMemcpyHostToDevice),
+           "nbk_set_replicas");
+  NBK_CUDA(cudaMemcpy(h->repLJ.p, t.data(), sizeof(float2) * t.size(), cudaMemcpyHostToDevice), "nbk_set_replicas");
+  NBK_CUDA(cudaMemcpy(h->repLJExcl.p, te.data(), sizeof(float2) * te.size(), cudaMemcpyHostToDevice),
+           "nbk_set_replicas");
+  NBK_CUDA(cudaMemsetAsync(h->acc.p, 0, sizeof(long long) * kAccCount * (size_t)numReplicas, st),
+           "nbk_set_replicas");
+  h->nrep = numReplicas;
+  h->slotRepSize = n;
+  h->built = h->refined = false;
+  return NBK_OK;
+}
+
+NBK_API int nbk_reduce_virial_energy_batch(nbk_handle h, unsigned flags, nbk_virial_energy* ve,
+                                           int veOnDevice, void* stream) {
+  int rc = checkHandle(h, "nbk_reduce_virial_energy_batch");
+  if (rc) return rc;
+  (void)flags;
+  if (!ve) return setErr(NBK_ERR_ARG, "nbk_reduce_virial_energy_batch: NULL output");
+  const int nr = h->nrep > 0 ? h->nrep : 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  nbk_virial_energy* dst = veOnDevice ? ve : h->ve.p;
+  NBK_CUDA(h->ve.ensure(nr), "nbk_reduce_virial_energy_batch");
+  dst = veOnDevice ? ve : h->ve.p;
+  NBK_CUDA(launchEnergyVirial(h->acc.p, dst, st, nr), "energy/virial read-out");
+  h->launches += 1;
+  if (!veOnDevice)
+    NBK_CUDA(cudaMemcpyAsync(ve, h->ve.p, sizeof(nbk_virial_energy) * nr, cudaMemcpyDeviceToHost, st),
+             "nbk_reduce_virial_energy_batch: D2H");
+  return NBK_OK;
+}
+
+NBK_API int nbk_get_pair_counts(nbk_handle h, long long* counts, int maxCount, void* stream) {
+  int rc = checkHandle(h, "nbk_get_pair_counts");
+  if (rc) return rc;
+  if (!counts || maxCount <= 0) return setErr(NBK_ERR_ARG, "nbk_get_pair_counts: bad output");
+  if (!(h->lastFlags & NBK_ENERGY))
+    return setErr(NBK_ERR_STATE, "nbk_get_pair_counts: the last evaluation did not compute energies");
+  const int nr = h->nrep > 0 ? h->nrep : 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<long long> accHost((size_t)kAccCount * nr);
+  NBK_CUDA(cudaMemcpyAsync(accHost.data(), h->acc.p, sizeof(long long) * accHost.size(),
+                           cudaMemcpyDeviceToHost, st), "nbk_get_pair_counts");
+  NBK_CUDA(cudaStreamSynchronize(st), "nbk_get_pair_counts");
+  for (int r = 0; r < nr && r < maxCount; ++r) counts[r] = accHost[(size_t)r * kAccCount + kAccNumPairs];
   return NBK_OK;
 }
 
@@ -706,9 +895,14 @@ NBK_API int nbk_get_pair_count(nbk_handle h, long long* pairs, void* stream) {
   if (!(h->lastFlags & NBK_ENERGY))
     return setErr(NBK_ERR_STATE, "nbk_get_pair_count: the last evaluation did not compute energies");
   cudaStream_t st = (cudaStream_t)stream;
-  NBK_CUDA(cudaMemcpyAsync(pairs, h->acc.p + kAccNumPairs, sizeof(long long), cudaMemcpyDeviceToHost, st),
-           "nbk_get_pair_count");
+  const int nr = h->nrep > 0 ? h->nrep : 1;
+  std::vector<long long> accHost((size_t)kAccCount * nr);
+  NBK_CUDA(cudaMemcpyAsync(accHost.data(), h->acc.p, sizeof(long long) * accHost.size(),
+                           cudaMemcpyDeviceToHost, st), "nbk_get_pair_count");
   NBK_CUDA(cudaStreamSynchronize(st), "nbk_get_pair_count");
+  long long tot = 0;
+  for (int r = 0; r < nr; ++r) tot += accHost[(size_t)r * kAccCount + kAccNumPairs];
+  *pairs = tot;
   return NBK_OK;
 }
 

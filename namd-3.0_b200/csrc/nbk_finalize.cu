@@ -12,16 +12,63 @@ namespace nbk {
 //     fast Coulomb and of the smooth (3 - r^2/rc^2)/(2 rc) part of the slow one
 //   excluded: slow -qq erf(beta r)/r
 // Both only within the cutoff, as the reference.
+// Adds a thread's energy/virial accumulators (slots 0..20) to one replica's
+// block: warp-reduced when the whole warp holds the same replica, else per thread.
+__device__ __forceinline__ void flushThreadAcc(long long* accBase, int rep, long long* acc) {
+  const int lane = threadIdx.x & 31;
+  const int rep0 = __shfl_sync(0xffffffffu, rep, 0);
+  const bool uniform = __all_sync(0xffffffffu, rep == rep0);
+#pragma unroll
+  for (int p = 0; p < kAccCount - 3; ++p) {
+    if (uniform) {
+      const long long v = warpSumLL(acc[p]);
+      if (lane == 0 && v != 0) atomicAddFixed(&accBase[(size_t)rep0 * kAccCount + p], (unsigned long long)v);
+    } else if (acc[p] != 0) {
+      atomicAddFixed(&accBase[(size_t)rep * kAccCount + p], (unsigned long long)acc[p]);
+    }
+    acc[p] = 0;
+  }
+}
+
 template <bool doEnergy, bool doVirial, bool doSlow, bool doE64>
 __global__ void correctionsKernel(const CorrArgs a) {
   const NbkConst& c = a.c;
   const int total = a.numModified + (doSlow ? a.numExcluded : 0);
   long long acc[kAccCount - 3] = {};  // energies + virials, thread-local
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+  // each warp owns a contiguous range of tuples (lanes interleaved), so its
+  // tuples belong to one replica except at replica boundaries
+  const int lane = threadIdx.x & 31;
+  const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int per = ((total + warpsTotal - 1) / warpsTotal + 31) & ~31;
+  const int kEnd = min(total, (gw + 1) * per);
+  int curRep = 0;
+  for (int k0 = gw * per; k0 < kEnd; k0 += 32) {
+    const int k = k0 + lane;
+    const bool valid = k < kEnd;
     const bool modified = k < a.numModified;
-    const nbk_exclusion e = modified ? a.modified[k] : a.excluded[k - a.numModified];
-    const float3 sh = shiftOf(make_float3(e.ioffsetXYZ.x, e.ioffsetXYZ.y, e.ioffsetXYZ.z), a.lata,
-                              a.latb, a.latc);
+    nbk_exclusion e{};
+    if (valid) e = modified ? a.modified[k] : a.excluded[k - a.numModified];
+    int rep = 0;
+    float3 la = a.lata, lb = a.latb, lc = a.latc;
+    const float2* ljx = a.ljExclTable;
+    if (a.slotRep && valid) {
+      rep = a.slotRep[e.i];
+      la = a.repLat[3 * rep];
+      lb = a.repLat[3 * rep + 1];
+      lc = a.repLat[3 * rep + 2];
+      ljx = a.repLJExcl + (size_t)rep * c.ljDim * c.ljDim;
+    }
+    if ((doEnergy || doVirial) && a.slotRep) {
+      // a warp-wide replica change flushes the accumulators first
+      const bool change = valid && rep != curRep;
+      if (__any_sync(0xffffffffu, change)) {
+        flushThreadAcc(a.acc, curRep, acc);
+        curRep = valid ? rep : curRep;
+      }
+    }
+    if (!valid) continue;
+    const float3 sh = shiftOf(make_float3(e.ioffsetXYZ.x, e.ioffsetXYZ.y, e.ioffsetXYZ.z), la, lb, lc);
     const float4 xi = a.xyzq[e.i];
     const float4 xj = a.xyzq[e.j];
     // d = x_j - (x_i + shift): the nonbonded kernel's sign convention
@@ -36,7 +83,7 @@ __global__ void correctionsKernel(const CorrArgs a) {
     const float qq = xi.w * xj.w;
     float g = 0.f, gs = 0.f, eV = 0.f, eE = 0.f, eS = 0.f;
     if (modified) {
-      const float2 ab = a.ljExclTable[e.vdwtypei * c.ljDim + e.vdwtypej];
+      const float2 ab = ljx[e.vdwtypei * c.ljDim + e.vdwtypej];
       const float rinv6 = rinv2 * rinv2 * rinv2;
       const float ab6 = fmaf(ab.x, rinv6, -ab.y);
       const float w = ab6 * rinv6;
@@ -110,16 +157,16 @@ __global__ void correctionsKernel(const CorrArgs a) {
       const double S0 = (double)e.ioffsetXYZ.x, S1 = (double)e.ioffsetXYZ.y,
                    S2 = (double)e.ioffsetXYZ.z;
       const double d[3] = {
-          (double)xj.x - ((double)xi.x + (S0 * a.lata.x + S1 * a.latb.x + S2 * a.latc.x)),
-          (double)xj.y - ((double)xi.y + (S0 * a.lata.y + S1 * a.latb.y + S2 * a.latc.y)),
-          (double)xj.z - ((double)xi.z + (S0 * a.lata.z + S1 * a.latb.z + S2 * a.latc.z))};
+          (double)xj.x - ((double)xi.x + (S0 * la.x + S1 * lb.x + S2 * lc.x)),
+          (double)xj.y - ((double)xi.y + (S0 * la.y + S1 * lb.y + S2 * lc.y)),
+          (double)xj.z - ((double)xi.z + (S0 * la.z + S1 * lb.z + S2 * lc.z))};
       const double r2d = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
       const double ri = rsqrt(r2d), ri2 = ri * ri, ri3 = ri * ri2;
       const double qqd = (double)xi.w * (double)xj.w;
       const NbkConst64& k = a.c64;
       double gd = 0.0, gsd = 0.0, eVd = 0.0, eEd = 0.0, eSd = 0.0;
       if (modified) {
-        const float2 ab = a.ljExclTable[e.vdwtypei * c.ljDim + e.vdwtypej];
+        const float2 ab = ljx[e.vdwtypei * c.ljDim + e.vdwtypej];
         const double ri6 = ri2 * ri2 * ri2;
         const double ab6 = fma((double)ab.x, ri6, -(double)ab.y);
         const double w = ab6 * ri6;
@@ -177,13 +224,7 @@ __global__ void correctionsKernel(const CorrArgs a) {
       }
     }
   }
-  if (doEnergy || doVirial) {
-#pragma unroll
-    for (int p = 0; p < kAccCount - 3; ++p) {
-      long long v = warpSumLL(acc[p]);
-      if ((threadIdx.x & 31) == 0 && v != 0) atomicAddFixed(&a.acc[p], (unsigned long long)v);
-    }
-  }
+  if (doEnergy || doVirial) flushThreadAcc(a.acc, a.slotRep ? curRep : 0, acc);
 }
 
 cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st) {
@@ -220,13 +261,35 @@ cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st
 // src/CudaComputeNonbondedKernel.cu:2057-2072) and the per-atom part of the
 // virial, sum_i F_i (x) x_i over patch-centred positions
 // (reduceNonbondedVirialKernel, :1649-1763), folded into fixed point per atom.
+// Each warp owns a contiguous slot range so that, with batched replicas, its
+// slots belong to one replica except at boundaries.
 __global__ void finalizeKernel(int n, const long long* __restrict__ F, int stride,
                                const float4* __restrict__ xyzq, float4* __restrict__ outF,
                                float4* __restrict__ outS, int doSlow, int doVirial,
-                               long long* __restrict__ acc) {
-  __shared__ long long s_v[32][18];
+                               long long* __restrict__ accBase, const int* __restrict__ slotRep) {
   long long v[18] = {};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int per = ((n + warpsTotal - 1) / warpsTotal + 31) & ~31;
+  const int iEnd = min(n, (gw + 1) * per);
+  int curRep = 0;
+  for (int i0 = gw * per; i0 < iEnd; i0 += 32) {
+    const int i = i0 + lane;
+    const bool valid = i < iEnd;
+    if (doVirial && slotRep) {
+      const int rep = valid ? slotRep[i] : curRep;
+      if (__any_sync(0xffffffffu, rep != curRep)) {
+        // flush per thread into the replica it accumulated for
+#pragma unroll
+        for (int p = 0; p < 18; ++p) {
+          if (v[p] != 0) atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
+          v[p] = 0;
+        }
+        curRep = rep;
+      }
+    }
+    if (!valid) continue;
     const long long fx = F[i], fy = F[stride + i], fz = F[2 * (size_t)stride + i];
     long long gx = 0, gy = 0, gz = 0;
     if (doSlow) {
@@ -253,24 +316,23 @@ __global__ void finalizeKernel(int n, const long long* __restrict__ F, int strid
     }
   }
   if (!doVirial) return;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int rep0 = __shfl_sync(0xffffffffu, curRep, 0);
+  const bool uniform = __all_sync(0xffffffffu, curRep == rep0);
 #pragma unroll
   for (int p = 0; p < 18; ++p) {
-    const long long s = warpSumLL(v[p]);
-    if (lane == 0) s_v[w][p] = s;
-  }
-  __syncthreads();
-  if (threadIdx.x < 18) {
-    long long t = 0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += s_v[k][threadIdx.x];
-    if (threadIdx.x >= 9 && !doSlow) t = 0;
-    if (t != 0) atomicAddFixed(&acc[kAccVir + threadIdx.x], (unsigned long long)t);
+    if (p >= 9 && !doSlow) break;
+    if (uniform) {
+      const long long s = warpSumLL(v[p]);
+      if (lane == 0 && s != 0) atomicAddFixed(&accBase[(size_t)rep0 * kAccCount + kAccVir + p], (unsigned long long)s);
+    } else if (v[p] != 0) {
+      atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
+    }
   }
 }
 
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
-                                 int numSM, cudaStream_t st) {
+                                 int numSM, cudaStream_t st, const int* slotRep) {
   if (n <= 0) return cudaSuccess;
   const bool V = flags & NBK_VIRIAL;
   if (!V && !outF && !outS) return cudaSuccess;
@@ -280,12 +342,15 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
   const bool atomVirial = V && !((flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64));
   if (!atomVirial && !outF && !outS) return cudaSuccess;
   finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS,
-                                             (flags & NBK_SLOW) ? 1 : 0, atomVirial ? 1 : 0, acc);
+                                             (flags & NBK_SLOW) ? 1 : 0, atomVirial ? 1 : 0, acc,
+                                             slotRep);
   return cudaGetLastError();
 }
 
-__global__ void energyVirialKernel(const long long* __restrict__ acc, nbk_virial_energy* out) {
+__global__ void energyVirialKernel(const long long* __restrict__ accBase, nbk_virial_energy* outBase) {
   const int t = threadIdx.x;
+  const long long* acc = accBase + (size_t)blockIdx.x * kAccCount;
+  nbk_virial_energy* out = outBase + blockIdx.x;
   double* o = reinterpret_cast<double*>(out);
   const int nd = (int)(sizeof(nbk_virial_energy) / sizeof(double));
   if (t < nd) o[t] = 0.0;
@@ -301,8 +366,9 @@ __global__ void energyVirialKernel(const long long* __restrict__ acc, nbk_virial
   }
 }
 
-cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st) {
-  energyVirialKernel<<<1, 32, 0, st>>>(acc, out);
+cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st,
+                               int numReplicas) {
+  energyVirialKernel<<<numReplicas, 32, 0, st>>>(acc, out);
   return cudaGetLastError();
 }
 

@@ -22,7 +22,35 @@ constexpr int kForceThreads = kForceWarps * kWarp;
 
 constexpr int kForceMinBlocks = 8;  // caps registers at 64 -> 32 warps per SM
 
-template <bool doEnergy, bool doVirial, bool doSlow, bool doPairlist, bool doE64>
+// Adds a warp's fixed-point accumulators to one replica's accumulator block.
+template <bool doEnergy, bool doVirial, bool doPairlist>
+__device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& accE0,
+                                          long long& accE1, long long& accE2, long long& accVir,
+                                          int& nexcl, int& npair) {
+  if (doVirial && lane < 18 && accVir != 0)
+    atomicAddFixed(&acc[kAccVir + lane], (unsigned long long)accVir);
+  if (doEnergy && lane == 0) {
+    if (accE0) atomicAddFixed(&acc[kAccEVdw], (unsigned long long)accE0);
+    if (accE1) atomicAddFixed(&acc[kAccEElec], (unsigned long long)accE1);
+    if (accE2) atomicAddFixed(&acc[kAccESlow], (unsigned long long)accE2);
+  }
+  if (doPairlist) {
+    int s = nexcl;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0 && s) atomicAddFixed(&acc[kAccNumExcl], (unsigned long long)s);
+  }
+  if (doEnergy) {
+    int s = npair;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0 && s) atomicAddFixed(&acc[kAccNumPairs], (unsigned long long)s);
+  }
+  accE0 = accE1 = accE2 = accVir = 0;
+  nexcl = npair = 0;
+}
+
+template <bool doEnergy, bool doVirial, bool doSlow, bool doPairlist, bool doE64, bool doBatch>
 __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
@@ -34,8 +62,10 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
   const int wib = threadIdx.x >> 5;
   const NbkConst& c = a.c;
   const int dim = c.ljDim;
-  for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) s_lj[k] = a.ljTable[k];
-  __syncthreads();
+  if (!doBatch) {
+    for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) s_lj[k] = a.ljTable[k];
+    __syncthreads();
+  }
 
   const int numLists = a.numListsDev ? *a.numListsDev : a.numListsHost;
 
@@ -44,6 +74,7 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
   long long accE0 = 0, accE1 = 0, accE2 = 0, accVir = 0;
   int nexcl = 0;
   int npair = 0;  // interacting pairs seen by this lane (energy evaluations)
+  int curRep = 0;  // replica whose accumulators the warp is holding
 
   // lists are handed out one at a time from a global counter, so warps that
   // draw short lists keep working instead of idling at the end
@@ -54,8 +85,22 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
     if (L >= numLists) break;
     const nbk_tile_list tl = a.lists[L];
     if (tl.jtileEnd < tl.jtileStart) continue;  // empty (warp-uniform)
+    float3 la = a.lata, lb = a.latb, lc = a.latc;
+    const float2* ljRow = nullptr;  // batched: this replica's LJ table (global)
+    if (doBatch) {
+      const int rep = __ldg(&a.compRep[tl.icompute]);
+      if (rep != curRep) {
+        flushWarp<doEnergy, doVirial, doPairlist>(a.acc + (size_t)curRep * kAccCount, lane, accE0,
+                                                  accE1, accE2, accVir, nexcl, npair);
+        curRep = rep;
+      }
+      la = a.repLat[3 * rep];
+      lb = a.repLat[3 * rep + 1];
+      lc = a.repLat[3 * rep + 2];
+      ljRow = a.repLJ + (size_t)rep * dim * dim;
+    }
     const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
-    const float3 sh = shiftOf(off, a.lata, a.latb, a.latc);
+    const float3 sh = shiftOf(off, la, lb, lc);
     const bool zeroShift = !(dist2(sh.x, sh.y, sh.z) > 0.0f);
     const bool selfCompute = (tl.patchInd.x == tl.patchInd.y) && zeroShift;
 
@@ -65,9 +110,9 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
     // from the FP32 offsets and lattice, without the FP32 rounding of sh
     double xid = 0.0, yid = 0.0, zid = 0.0;
     if (doE64) {
-      xid = (double)xi.x + ((double)off.x * a.lata.x + (double)off.y * a.latb.x + (double)off.z * a.latc.x);
-      yid = (double)xi.y + ((double)off.x * a.lata.y + (double)off.y * a.latb.y + (double)off.z * a.latc.y);
-      zid = (double)xi.z + ((double)off.x * a.lata.z + (double)off.y * a.latb.z + (double)off.z * a.latc.z);
+      xid = (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x);
+      yid = (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y);
+      zid = (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z);
     }
     xi.x = __fadd_rn(xi.x, sh.x);
     xi.y = __fadd_rn(xi.y, sh.y);
@@ -165,7 +210,7 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
         }
         if (active) {
           if (doEnergy) ++npair;
-          const float2 ab = s_lj[ti + s_type[wib][j]];
+          const float2 ab = doBatch ? __ldg(&ljRow[ti + s_type[wib][j]]) : s_lj[ti + s_type[wib][j]];
           float f, fs;
           pairForce<doEnergy, doSlow>(r2, xi.w * xjj.w, ab, c, f, fs, eVt, eEt, eSt);
           if (doE64) {
@@ -315,31 +360,14 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
 
   // per-warp flush of the fixed-point accumulators (no block barrier, so a
   // warp that runs out of lists retires at once)
-  if (doVirial && lane < 18 && accVir != 0)
-    atomicAddFixed(&a.acc[kAccVir + lane], (unsigned long long)accVir);
-  if (doEnergy && lane == 0) {
-    if (accE0) atomicAddFixed(&a.acc[kAccEVdw], (unsigned long long)accE0);
-    if (accE1) atomicAddFixed(&a.acc[kAccEElec], (unsigned long long)accE1);
-    if (accE2) atomicAddFixed(&a.acc[kAccESlow], (unsigned long long)accE2);
-  }
-  if (doPairlist) {
-    int s = nexcl;
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0 && s) atomicAddFixed(&a.acc[kAccNumExcl], (unsigned long long)s);
-  }
-  if (doEnergy) {
-    int s = npair;
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0 && s) atomicAddFixed(&a.acc[kAccNumPairs], (unsigned long long)s);
-  }
+  flushWarp<doEnergy, doVirial, doPairlist>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1,
+                                            accE2, accVir, nexcl, npair);
 }
 
-template <bool E, bool V, bool S, bool P, bool D>
+template <bool E, bool V, bool S, bool P, bool D, bool B>
 static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
-  const size_t shmem = sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
-  auto k = forceKernel<E, V, S, P, D>;
+  const size_t shmem = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
+  auto k = forceKernel<E, V, S, P, D, B>;
   static int cachedDim = -1, cachedBlocks = 0;
   if (cachedDim != a.c.ljDim) {
     if (shmem > 48 * 1024) {
@@ -358,36 +386,55 @@ static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
 
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st) {
   const bool E = flags & NBK_ENERGY;
-  const int idx = (E ? 16 : 0) | ((flags & NBK_VIRIAL) ? 8 : 0) | ((flags & NBK_SLOW) ? 4 : 0) |
-                  ((flags & NBK_PAIRLIST) ? 2 : 0) | ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
+  const bool B = a.compRep != nullptr;
+  const int idx = (B ? 32 : 0) | (E ? 16 : 0) | ((flags & NBK_VIRIAL) ? 8 : 0) |
+                  ((flags & NBK_SLOW) ? 4 : 0) | ((flags & NBK_PAIRLIST) ? 2 : 0) |
+                  ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
   switch (idx) {
-#define NBK_CASE(i, e, v, s, p, d) \
-  case i:                          \
-    return launchT<e, v, s, p, d>(a, numSM, st);
-    NBK_CASE(0, false, false, false, false, false)
-    NBK_CASE(2, false, false, false, true, false)
-    NBK_CASE(4, false, false, true, false, false)
-    NBK_CASE(6, false, false, true, true, false)
-    NBK_CASE(8, false, true, false, false, false)
-    NBK_CASE(10, false, true, false, true, false)
-    NBK_CASE(12, false, true, true, false, false)
-    NBK_CASE(14, false, true, true, true, false)
-    NBK_CASE(16, true, false, false, false, false)
-    NBK_CASE(17, true, false, false, false, true)
-    NBK_CASE(18, true, false, false, true, false)
-    NBK_CASE(19, true, false, false, true, true)
-    NBK_CASE(20, true, false, true, false, false)
-    NBK_CASE(21, true, false, true, false, true)
-    NBK_CASE(22, true, false, true, true, false)
-    NBK_CASE(23, true, false, true, true, true)
-    NBK_CASE(24, true, true, false, false, false)
-    NBK_CASE(25, true, true, false, false, true)
-    NBK_CASE(26, true, true, false, true, false)
-    NBK_CASE(27, true, true, false, true, true)
-    NBK_CASE(28, true, true, true, false, false)
-    NBK_CASE(29, true, true, true, false, true)
-    NBK_CASE(30, true, true, true, true, false)
-    NBK_CASE(31, true, true, true, true, true)
+#define NBK_CASE(i, e, v, s, p, d, b) \
+  case i:                             \
+    return launchT<e, v, s, p, d, b>(a, numSM, st);
+    NBK_CASE(0, false, false, false, false, false, false)
+    NBK_CASE(2, false, false, false, true, false, false)
+    NBK_CASE(4, false, false, true, false, false, false)
+    NBK_CASE(6, false, false, true, true, false, false)
+    NBK_CASE(8, false, true, false, false, false, false)
+    NBK_CASE(10, false, true, false, true, false, false)
+    NBK_CASE(12, false, true, true, false, false, false)
+    NBK_CASE(14, false, true, true, true, false, false)
+    NBK_CASE(16, true, false, false, false, false, false)
+    NBK_CASE(17, true, false, false, false, true, false)
+    NBK_CASE(18, true, false, false, true, false, false)
+    NBK_CASE(19, true, false, false, true, true, false)
+    NBK_CASE(20, true, false, true, false, false, false)
+    NBK_CASE(21, true, false, true, false, true, false)
+    NBK_CASE(22, true, false, true, true, false, false)
+    NBK_CASE(23, true, false, true, true, true, false)
+    NBK_CASE(24, true, true, false, false, false, false)
+    NBK_CASE(25, true, true, false, false, true, false)
+    NBK_CASE(26, true, true, false, true, false, false)
+    NBK_CASE(27, true, true, false, true, true, false)
+    NBK_CASE(28, true, true, true, false, false, false)
+    NBK_CASE(29, true, true, true, false, true, false)
+    NBK_CASE(30, true, true, true, true, false, false)
+    NBK_CASE(31, true, true, true, true, true, false)
+    // batched replicas (FP32 energy mode)
+    NBK_CASE(32, false, false, false, false, false, true)
+    NBK_CASE(34, false, false, false, true, false, true)
+    NBK_CASE(36, false, false, true, false, false, true)
+    NBK_CASE(38, false, false, true, true, false, true)
+    NBK_CASE(40, false, true, false, false, false, true)
+    NBK_CASE(42, false, true, false, true, false, true)
+    NBK_CASE(44, false, true, true, false, false, true)
+    NBK_CASE(46, false, true, true, true, false, true)
+    NBK_CASE(48, true, false, false, false, false, true)
+    NBK_CASE(50, true, false, false, true, false, true)
+    NBK_CASE(52, true, false, true, false, false, true)
+    NBK_CASE(54, true, false, true, true, false, true)
+    NBK_CASE(56, true, true, false, false, false, true)
+    NBK_CASE(58, true, true, false, true, false, true)
+    NBK_CASE(60, true, true, true, false, false, true)
+    NBK_CASE(62, true, true, true, true, false, true)
 #undef NBK_CASE
   }
   return cudaErrorInvalidValue;

@@ -247,6 +247,10 @@ struct ForceArgs {
   long long* acc;              // [kAccCount]
   int* workCounter;            // next list to hand out (zeroed before the launch)
   NbkConst64 c64;              // FP64 energy/virial mode
+  // replicas (batched evaluation; all NULL for a single system)
+  const int* compRep;          // [numComputes] replica of each compute
+  const float3* repLat;        // [3*numReplicas] lattice vectors a, b, c
+  const float2* repLJ;         // [numReplicas][ljDim*ljDim] (A, B) * scaling
 };
 
 }  // namespace nbk

@@ -14,8 +14,9 @@ cudaError_t launchBBoxes(int numTiles, const float4* xyzq, BBox* bb, cudaStream_
 cudaError_t launchBuildLists(int numLists, const ListSeed* seeds,
                              const nbk_compute_record* computes, const nbk_patch_record* patches,
                              const BBox* bb, float3 lata, float3 latb, float3 latc,
-                             float plcutoff2Culling, nbk_tile_list* lists, PatchPair* pp,
-                             int* tileJatomStart, cudaStream_t st);
+                             const int* compRep, const float3* repLat, float plcutoff2Culling,
+                             nbk_tile_list* lists, PatchPair* pp, int* tileJatomStart,
+                             cudaStream_t st);
 
 cudaError_t launchCompact(int numLists, const nbk_tile_list* src, const int* listActive,
                           const int* jtileActive, const int* jatomSrc, const nbk_tile_excl* exclSrc,
@@ -35,13 +36,41 @@ struct CorrArgs {
   int stride;
   long long* acc;
   NbkConst64 c64;
+  // replicas (batched evaluation; NULL for a single system)
+  const int* slotRep;          // [atomStorageSize] replica of each atom slot
+  const float3* repLat;        // [3*numReplicas]
+  const float2* repLJExcl;     // [numReplicas][ljDim*ljDim] (A14 - A, B14 - B) * scaling
 };
 cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st);
 
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
-                                 int numSM, cudaStream_t st);
+                                 int numSM, cudaStream_t st, const int* slotRep = nullptr);
 
-cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st);
+// Converts numReplicas accumulator blocks into numReplicas nbk_virial_energy records.
+cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st,
+                               int numReplicas = 1);
+
+struct AdjArgs {
+  const nbk_tile_list* lists;
+  const int* numListsDev;
+  const int* tileJatomStart;
+  const nbk_tile_excl* tileExcls;
+  const float4* xyzq;
+  const int* vdwTypes;
+  const float2* ljTable;
+  const int* typeMask;   // [ljDim] 1: accumulate LJ gradients of pairs touching this type
+  const float4* wF;      // fast-force cotangent per slot (w ignored)
+  const float4* wS;      // slow-force cotangent per slot (NULL: zero)
+  float cV, cE, cS;
+  float3 lata, latb, latc;
+  NbkConst c;
+  long long* grad;       // SoA [4][stride]: gx, gy, gz, gq (fixed point, force scale)
+  int stride;
+  double* gradAB;        // [2][ljDim*ljDim] (FP64 atomics)
+  int* workCounter;
+};
+cudaError_t launchAdjoint(const AdjArgs& a, bool doSlow, int numSM, int n, float4* out,
+                          cudaStream_t st);
 
 }  // namespace nbk

@@ -58,6 +58,7 @@ __global__ void buildListsKernel(int numLists, const ListSeed* __restrict__ seed
                                  const nbk_compute_record* __restrict__ computes,
                                  const nbk_patch_record* __restrict__ patches,
                                  const BBox* __restrict__ bb, float3 lata, float3 latb, float3 latc,
+                                 const int* __restrict__ compRep, const float3* __restrict__ repLat,
                                  float cull2, nbk_tile_list* __restrict__ lists,
                                  PatchPair* __restrict__ pp, int* __restrict__ tileJatomStart) {
   const int lane = threadIdx.x & 31;
@@ -67,8 +68,14 @@ __global__ void buildListsKernel(int numLists, const ListSeed* __restrict__ seed
     const nbk_compute_record cr = computes[sd.icompute];
     const nbk_patch_record p1 = patches[cr.patchInd.x];
     const nbk_patch_record p2 = patches[cr.patchInd.y];
-    const float3 sh = shiftOf(make_float3(cr.offsetXYZ.x, cr.offsetXYZ.y, cr.offsetXYZ.z), lata,
-                              latb, latc);
+    float3 la = lata, lb = latb, lc = latc;
+    if (compRep) {  // batched replicas: this compute's replica lattice
+      const int rep = compRep[sd.icompute];
+      la = repLat[3 * rep];
+      lb = repLat[3 * rep + 1];
+      lc = repLat[3 * rep + 2];
+    }
+    const float3 sh = shiftOf(make_float3(cr.offsetXYZ.x, cr.offsetXYZ.y, cr.offsetXYZ.z), la, lb, lc);
     const bool zeroShift = !(dist2(sh.x, sh.y, sh.z) > 0.0f);
     const bool self = zeroShift && (p1.atomStart == p2.atomStart);
     BBox bi = bb[p1.atomStart / 32 + sd.itile];
@@ -164,14 +171,16 @@ cudaError_t launchBBoxes(int numTiles, const float4* xyzq, BBox* bb, cudaStream_
 
 cudaError_t launchBuildLists(int numLists, const ListSeed* seeds,
                              const nbk_compute_record* computes, const nbk_patch_record* patches,
-                             const BBox* bb, float3 lata, float3 latb, float3 latc, float cull2,
+                             const BBox* bb, float3 lata, float3 latb, float3 latc,
+                             const int* compRep, const float3* repLat, float cull2,
                              nbk_tile_list* lists, PatchPair* pp, int* tileJatomStart,
                              cudaStream_t st) {
   if (numLists <= 0) return cudaSuccess;
   const int threads = 256;
   const int blocks = min((numLists + 7) / 8, 8192);
   buildListsKernel<<<blocks, threads, 0, st>>>(numLists, seeds, computes, patches, bb, lata, latb,
-                                               latc, cull2, lists, pp, tileJatomStart);
+                                               latc, compRep, repLat, cull2, lists, pp,
+                                               tileJatomStart);
   return cudaGetLastError();
 }
 

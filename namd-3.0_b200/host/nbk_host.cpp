@@ -195,6 +195,10 @@ struct nbk_packed_s {
   std::vector<double> centers;
   std::vector<std::vector<int>> patchAtoms;  // slot order of each patch
   std::vector<std::pair<int, int>> modPairsGlobal, exclPairsGlobal;
+  // replicas: a single packing is replica 0
+  std::vector<int> replicaOfCompute, replicaSlotStart, replicaAtomStart;
+  std::vector<nbk_float3> replicaLattice;
+  bool many = false;
 };
 
 extern "C" {
@@ -464,6 +468,38 @@ NBK_API int nbk_lj_table(int ntypes, const double* sigma, const double* epsilon,
   return NBK_OK;
 }
 
+// Chain rule from gradients w.r.t. the scaled LJ table entries (A*scaling,
+// B*scaling at ordered type pair (i, j)) to per-type sigma and epsilon, for the
+// combining rule of nbk_lj_table (LJTable::compute_vdw_params).
+NBK_API int nbk_lj_param_grad(int ntypes, const double* sigma, const double* epsilon, int geometric,
+                              double scaling, const double* gA, const double* gB, double* gSigma,
+                              double* gEps) {
+  if (ntypes <= 0 || !sigma || !epsilon || !gA || !gB || !gSigma || !gEps)
+    return fail(NBK_ERR_ARG, "nbk_lj_param_grad: bad argument");
+  for (int t = 0; t < ntypes; ++t) gSigma[t] = gEps[t] = 0.0;
+  for (int i = 0; i < ntypes; ++i)
+    for (int j = 0; j < ntypes; ++j) {
+      const double ga = gA[i * ntypes + j] * scaling, gb = gB[i * ntypes + j] * scaling;
+      if (ga == 0.0 && gb == 0.0) continue;
+      const double s = geometric ? std::sqrt(sigma[i] * sigma[j]) : 0.5 * (sigma[i] + sigma[j]);
+      const double e = std::sqrt(epsilon[i] * epsilon[j]);
+      const double s5 = s * s * s * s * s, s6 = s5 * s, s11 = s6 * s5, s12 = s6 * s6;
+      // A = 4 e s^12, B = 4 e s^6
+      const double dLds = ga * 48.0 * e * s11 + gb * 24.0 * e * s5;
+      const double dLde = ga * 4.0 * s12 + gb * 4.0 * s6;
+      // d s / d sigma_i (and _j), d e / d eps_i (and _j)
+      const double dsi = geometric ? (sigma[i] > 0 ? 0.5 * s / sigma[i] : 0.0) : 0.5;
+      const double dsj = geometric ? (sigma[j] > 0 ? 0.5 * s / sigma[j] : 0.0) : 0.5;
+      const double dei = epsilon[i] > 0 ? 0.5 * e / epsilon[i] : 0.0;
+      const double dej = epsilon[j] > 0 ? 0.5 * e / epsilon[j] : 0.0;
+      gSigma[i] += dLds * dsi;
+      gSigma[j] += dLds * dsj;
+      gEps[i] += dLde * dei;
+      gEps[j] += dLde * dej;
+    }
+  return NBK_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -710,6 +746,11 @@ NBK_API int nbk_pack(nbk_system S, double patchDim, double coulombScaling, nbk_p
     P->modified.push_back(makeTuple(P, S, S->modPairs[k], S->modPairs[k + 1]));
   }
 
+  P->replicaOfCompute.assign(P->computes.size(), 0);
+  P->replicaSlotStart = {0, storage};
+  P->replicaAtomStart = {0, S->natoms};
+  P->replicaLattice = {nbk_float3{(float)S->box[0], 0.f, 0.f}, nbk_float3{0.f, (float)S->box[1], 0.f},
+                       nbk_float3{0.f, 0.f, (float)S->box[2]}};
   nbk_packed_view& v = P->v;
   v.natoms = S->natoms;
   v.numPatches = np;
@@ -734,7 +775,113 @@ NBK_API int nbk_pack(nbk_system S, double patchDim, double coulombScaling, nbk_p
   v.excluded = P->excluded.empty() ? nullptr : P->excluded.data();
   v.slotOfAtom = P->slotOfAtom.data();
   v.patchCenter = P->centers.data();
+  v.numReplicas = 1;
+  v.replicaOfCompute = P->replicaOfCompute.data();
+  v.replicaSlotStart = P->replicaSlotStart.data();
+  v.replicaAtomStart = P->replicaAtomStart.data();
+  v.replicaLattice = P->replicaLattice.data();
   *out = P;
+  return NBK_OK;
+}
+
+NBK_API int nbk_pack_many(const nbk_system* systems, int n, double patchDim, double coulombScaling,
+                          nbk_packed* out) {
+  if (!systems || n <= 0 || !out) return fail(NBK_ERR_ARG, "nbk_pack_many: bad argument");
+  nbk_packed_s* M = new (std::nothrow) nbk_packed_s;
+  if (!M) return fail(NBK_ERR_NOMEM, "nbk_pack_many: out of memory");
+  M->many = true;
+  int slotOff = 0, patchOff = 0, atomOff = 0, maxTiles = 0;
+  long long bitOff = 0;
+  M->replicaSlotStart.push_back(0);
+  M->replicaAtomStart.push_back(0);
+  for (int r = 0; r < n; ++r) {
+    nbk_packed one = nullptr;
+    int rc = nbk_pack(systems[r], patchDim, coulombScaling, &one);
+    if (rc) {
+      delete M;
+      return rc;
+    }
+    const nbk_packed_view& v = one->v;
+    for (int p = 0; p < v.numPatches; ++p) {
+      nbk_patch_record pr = one->patches[p];
+      pr.atomStart += slotOff;
+      pr.patchID += patchOff;
+      M->patches.push_back(pr);
+      for (int d = 0; d < 3; ++d) M->centers.push_back(one->centers[3 * p + d]);
+    }
+    for (const nbk_compute_record& c : one->computes) {
+      nbk_compute_record cc = c;
+      cc.patchInd.x += patchOff;
+      cc.patchInd.y += patchOff;
+      M->computes.push_back(cc);
+      M->replicaOfCompute.push_back(r);
+    }
+    for (int k = 0; k < v.atomStorageSize; ++k) {
+      M->xyzq.push_back(one->xyzq[k]);
+      M->vdwTypes.push_back(one->vdwTypes[k]);
+      M->atomIndex.push_back(one->atomIndex[k] + atomOff);
+      nbk_int2 e = one->exclIndexMaxDiff[k];
+      e.x += (int)bitOff;
+      M->exclIndexMaxDiff.push_back(e);
+    }
+    for (unsigned w : one->bits) M->bits.push_back(w);
+    for (int a = 0; a < v.natoms; ++a) M->slotOfAtom.push_back(one->slotOfAtom[a] + slotOff);
+    for (nbk_exclusion e : one->modified) {
+      e.i += slotOff;
+      e.j += slotOff;
+      M->modified.push_back(e);
+    }
+    for (nbk_exclusion e : one->excluded) {
+      e.i += slotOff;
+      e.j += slotOff;
+      M->excluded.push_back(e);
+    }
+    M->replicaLattice.push_back(v.lata);
+    M->replicaLattice.push_back(v.latb);
+    M->replicaLattice.push_back(v.latc);
+    maxTiles = std::max(maxTiles, v.maxTileListLen);
+    slotOff += v.atomStorageSize;
+    patchOff += v.numPatches;
+    atomOff += v.natoms;
+    bitOff += 32LL * (long long)one->bits.size();
+    M->replicaSlotStart.push_back(slotOff);
+    M->replicaAtomStart.push_back(atomOff);
+    nbk_packed_free(one);
+  }
+  if (bitOff > (1LL << 31)) {
+    delete M;
+    return fail(NBK_ERR_OVERFLOW, "nbk_pack_many: exclusion bit array exceeds 2^31 bits");
+  }
+  nbk_packed_view& v = M->v;
+  v.natoms = atomOff;
+  v.numPatches = patchOff;
+  v.patchGrid[0] = v.patchGrid[1] = v.patchGrid[2] = 0;
+  v.atomStorageSize = slotOff;
+  v.maxTileListLen = maxTiles;
+  v.numComputes = (int)M->computes.size();
+  v.numExclusionWords = (int)M->bits.size();
+  v.numModified = (int)M->modified.size();
+  v.numExcluded = (int)M->excluded.size();
+  v.lata = M->replicaLattice[0];
+  v.latb = M->replicaLattice[1];
+  v.latc = M->replicaLattice[2];
+  v.patches = M->patches.data();
+  v.computes = M->computes.data();
+  v.xyzq = M->xyzq.data();
+  v.vdwTypes = M->vdwTypes.data();
+  v.atomIndex = M->atomIndex.data();
+  v.exclIndexMaxDiff = M->exclIndexMaxDiff.data();
+  v.exclusionBits = M->bits.data();
+  v.modified = M->modified.empty() ? nullptr : M->modified.data();
+  v.excluded = M->excluded.empty() ? nullptr : M->excluded.data();
+  v.slotOfAtom = M->slotOfAtom.data();
+  v.patchCenter = M->centers.data();
+  v.numReplicas = n;
+  v.replicaOfCompute = M->replicaOfCompute.data();
+  v.replicaSlotStart = M->replicaSlotStart.data();
+  v.replicaAtomStart = M->replicaAtomStart.data();
+  v.replicaLattice = M->replicaLattice.data();
+  *out = M;
   return NBK_OK;
 }
 
@@ -745,6 +892,7 @@ NBK_API int nbk_packed_view_get(nbk_packed P, nbk_packed_view* v) {
 }
 
 NBK_API int nbk_pack_update_positions(nbk_packed P, nbk_system S) {
+  if (P && P->many) return fail(NBK_ERR_ARG, "nbk_pack_update_positions: not for nbk_pack_many layouts");
   if (!P || !S || S->natoms != P->v.natoms)
     return fail(NBK_ERR_ARG, "nbk_pack_update_positions: system does not match the packing");
   fillXyzq(P, S);

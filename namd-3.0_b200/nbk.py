@@ -102,7 +102,10 @@ class PackedView(C.Structure):
                 ("atomIndex", C.POINTER(C.c_int)), ("exclIndexMaxDiff", C.POINTER(Int2)),
                 ("exclusionBits", C.POINTER(C.c_uint)), ("modified", C.POINTER(Exclusion)),
                 ("excluded", C.POINTER(Exclusion)), ("slotOfAtom", C.POINTER(C.c_int)),
-                ("patchCenter", C.POINTER(C.c_double))]
+                ("patchCenter", C.POINTER(C.c_double)),
+                ("numReplicas", C.c_int), ("replicaOfCompute", C.POINTER(C.c_int)),
+                ("replicaSlotStart", C.POINTER(C.c_int)), ("replicaAtomStart", C.POINTER(C.c_int)),
+                ("replicaLattice", C.POINTER(Float3))]
 
 
 NBK_ENERGY, NBK_VIRIAL, NBK_SLOW, NBK_PAIRLIST, NBK_CORRECTIONS = 1, 2, 4, 8, 16
@@ -143,6 +146,10 @@ def host_lib() -> C.CDLL:
         lib.nbk_pack.argtypes = [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_void_p)]
         lib.nbk_packed_view_get.argtypes = [C.c_void_p, C.POINTER(PackedView)]
         lib.nbk_pack_update_positions.argtypes = [C.c_void_p, C.c_void_p]
+        lib.nbk_lj_param_grad.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        lib.nbk_pack_many.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_double,
+                                      C.POINTER(C.c_void_p)]
         lib.nbk_packed_free.argtypes = [C.c_void_p]
         _host = lib
     return _host
@@ -230,16 +237,46 @@ class System:
         return nt, A, B, A14, B14
 
 
-class Packed:
-    """Host mirror of CudaComputeNonbonded's inputs for one system."""
+def lj_param_grad(sigma, epsilon, gA, gB, scaling=1.0, geometric=False):
+    """Per-type (dL/dsigma, dL/depsilon) from gradients w.r.t. the scaled LJ
+    table entries (nbk_lj_param_grad)."""
+    nt = len(sigma)
+    sg = np.ascontiguousarray(sigma, dtype=np.float64)
+    ep = np.ascontiguousarray(epsilon, dtype=np.float64)
+    a = np.ascontiguousarray(gA, dtype=np.float64).reshape(-1)
+    b = np.ascontiguousarray(gB, dtype=np.float64).reshape(-1)
+    gs, ge = np.zeros(nt), np.zeros(nt)
+    _hcheck(host_lib().nbk_lj_param_grad(nt, sg.ctypes.data, ep.ctypes.data, int(geometric),
+                                         scaling, a.ctypes.data, b.ctypes.data, gs.ctypes.data,
+                                         ge.ctypes.data), "nbk_lj_param_grad")
+    return gs, ge
 
-    def __init__(self, system: System, patch_dim: float = 13.5, coulomb_scaling: float = 1.0):
+
+class Packed:
+    """Host mirror of CudaComputeNonbonded's inputs for one system, or for
+    several independent systems (replicas) concatenated (Packed.many)."""
+
+    def __init__(self, system: System, patch_dim: float = 13.5, coulomb_scaling: float = 1.0,
+                 _handle=None, _systems=None):
         lib = host_lib()
-        h = C.c_void_p()
-        _hcheck(lib.nbk_pack(system._h, patch_dim, coulomb_scaling, C.byref(h)), "nbk_pack")
+        if _handle is None:
+            h = C.c_void_p()
+            _hcheck(lib.nbk_pack(system._h, patch_dim, coulomb_scaling, C.byref(h)), "nbk_pack")
+            self.systems = [system]
+        else:
+            h = _handle
+            self.systems = list(_systems)
         self._h = h
-        self.system = system
+        self.system = self.systems[0]
         self._refresh()
+
+    @classmethod
+    def many(cls, systems, patch_dim: float = 13.5, coulomb_scaling: float = 1.0):
+        arr = (C.c_void_p * len(systems))(*[x._h for x in systems])
+        h = C.c_void_p()
+        _hcheck(host_lib().nbk_pack_many(arr, len(systems), patch_dim, coulomb_scaling,
+                                         C.byref(h)), "nbk_pack_many")
+        return cls(None, _handle=h, _systems=systems)
 
     def __del__(self):
         if getattr(self, "_h", None) and _host is not None:
@@ -272,6 +309,11 @@ class Packed:
                           ("off", np.float32, 3), ("pswitch", np.int32)])
         self.modified = _arr(v.modified, v.numModified * 32, np.uint8).view(ex_dt)
         self.excluded = _arr(v.excluded, v.numExcluded * 32, np.uint8).view(ex_dt)
+        self.numReplicas = v.numReplicas
+        self.replicaOfCompute = _arr(v.replicaOfCompute, v.numComputes, np.int32)
+        self.replicaSlotStart = _arr(v.replicaSlotStart, v.numReplicas + 1, np.int32)
+        self.replicaAtomStart = _arr(v.replicaAtomStart, v.numReplicas + 1, np.int32)
+        self.replicaLattice = _arr(v.replicaLattice, 9 * v.numReplicas, np.float32).reshape(-1, 3, 3)
 
     def update_positions(self):
         _hcheck(host_lib().nbk_pack_update_positions(self._h, self.system._h),
@@ -310,6 +352,11 @@ def dev_lib() -> C.CDLL:
         lib.nbk_launch_count.argtypes = [vp]
         lib.nbk_get_pair_count.argtypes = [vp, C.POINTER(C.c_longlong), vp]
         lib.nbk_measure_fp32_peak.argtypes = [i, C.POINTER(C.c_double)]
+        lib.nbk_set_replicas.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp]
+        lib.nbk_adjoint.argtypes = [vp, u, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp,
+                                    vp, vp]
+        lib.nbk_reduce_virial_energy_batch.argtypes = [vp, u, vp, i, vp]
+        lib.nbk_get_pair_counts.argtypes = [vp, C.POINTER(C.c_longlong), i, vp]
         _dev = lib
     return _dev
 
@@ -374,6 +421,59 @@ class Nonbonded:
                                            v.numExcluded, C.cast(v.excluded, C.c_void_p), stream),
                 "nbk_set_exclusion_tuples")
         self.packed = packed
+
+    def set_replicas(self, packed: Packed, stream=None):
+        """Batched mode: every replica of a Packed.many layout with its own
+        lattice and LJ tables (call after setup)."""
+        tabs = [x.lj_table() for x in packed.systems]
+        dims = {t[0] for t in tabs}
+        if len(dims) != 1:
+            raise NbkError("replicas must share the number of LJ types")
+        cat = [np.ascontiguousarray(np.concatenate([t[k] for t in tabs])) for k in (1, 2, 3, 4)]
+        self._rep_lj = cat
+        lat = np.ascontiguousarray(packed.replicaLattice.reshape(-1, 3), dtype=np.float32)
+        self._rep_lat = lat
+        roc = np.ascontiguousarray(packed.replicaOfCompute, dtype=np.int32)
+        rss = np.ascontiguousarray(packed.replicaSlotStart, dtype=np.int32)
+        self._rep_idx = (roc, rss)
+        _dcheck(dev_lib().nbk_set_replicas(self._h, packed.numReplicas, roc.ctypes.data,
+                                           rss.ctypes.data, lat.ctypes.data,
+                                           *(a.ctypes.data for a in cat), stream),
+                "nbk_set_replicas")
+        self.numReplicas = packed.numReplicas
+
+    def adjoint(self, wF, wS, cV, cE, cS, gradXQ, gradAB, type_mask=None, grad_fixed=None,
+                slow=True, stream=None):
+        """Gradient of sum wF.F + sum wS.Fslow + cV E_vdw + cE E_elec + cS E_slow
+        (nbk_adjoint). wF, wS, gradXQ: device float4[n]; gradAB: device double[2*dim*dim]."""
+        mask = None
+        if type_mask is not None:
+            mask = np.ascontiguousarray(type_mask, dtype=np.int32)
+        _dcheck(dev_lib().nbk_adjoint(self._h, NBK_SLOW if slow else 0, _ptr(wF), _ptr(wS),
+                                      cV, cE, cS, None if mask is None else mask.ctypes.data,
+                                      _ptr(gradXQ), _ptr(grad_fixed), _ptr(gradAB), stream),
+                "nbk_adjoint")
+
+    def virial_energy_batch(self, stream=None):
+        n = self.numReplicas
+        arr = (VirialEnergy * n)()
+        _dcheck(dev_lib().nbk_reduce_virial_energy_batch(self._h, NBK_ENERGY | NBK_VIRIAL | NBK_SLOW,
+                                                         C.cast(arr, C.c_void_p), 0, stream),
+                "nbk_reduce_virial_energy_batch")
+        import torch
+        torch.cuda.synchronize(self.device)
+        return list(arr)
+
+    def virial_energy_batch_to(self, ptr: int, on_device: bool, stream=None):
+        _dcheck(dev_lib().nbk_reduce_virial_energy_batch(self._h, NBK_ENERGY | NBK_VIRIAL | NBK_SLOW,
+                                                         ptr, int(on_device), stream),
+                "nbk_reduce_virial_energy_batch")
+
+    def pair_counts(self, stream=None):
+        n = getattr(self, "numReplicas", 1)
+        arr = (C.c_longlong * n)()
+        _dcheck(dev_lib().nbk_get_pair_counts(self._h, arr, n, stream), "nbk_get_pair_counts")
+        return np.array(arr[:], dtype=np.int64)
 
     def build_tile_lists(self, packed: Packed, xyzq=None, stream=None):
         """xyzq: None (host copy of packed.xyzq) or a device tensor."""

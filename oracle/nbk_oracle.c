@@ -455,3 +455,225 @@ void oracle_pair_modified(int n, const double* r2, const double* qq, const doubl
     out[5 * q + 4] = -qq[q] * h;
   }
 }
+
+/* ---- adjoint (config: L = sum wF.F_fast + sum wS.F_slow + cV E_vdw + cE E_elec + cS E_slow) ----
+ * Restated from the pair math above: with s = r^2, each pair contributes
+ *   l = pF g(s) + pS gs(s) + cV E_lj(s) + cE qq phi_f(s) + cS qq phi_s(s),
+ *   pF = (wF_i - wF_j).d, pS = (wS_i - wS_j).d, d = x_j - x_i,
+ * so dl/dd = g uF + gs uS + d [2 (pF g' + pS gs') + cV g_lj + cE qq g_f + cS qq g_s]
+ * (' = d/ds; 2 dE/ds = g for every term). */
+
+/* Second derivatives d/ds of the (dE/dr)/r functions, FP64. */
+static inline void pair_second(const pair_consts* k, double s, double A, double B, double* glj,
+                               double* dglj, double* gA, double* gB, double* EA, double* EB,
+                               double* gf, double* dgf, double* gsl, double* dgsl, double* phf,
+                               double* phs) {
+  const double si = 1.0 / s, s3 = si * si * si, s6 = s3 * s3;
+  /* W(s) = A s^-6 - B s^-3 */
+  const double WA = s6, WB = -s3;
+  const double WA1 = -6.0 * s6 * si, WB1 = 3.0 * s3 * si;
+  const double WA2 = 42.0 * s6 * si * si, WB2 = -12.0 * s3 * si * si;
+  double S = 1.0, S1 = 0.0, S2 = 0.0;
+  if (k->switching && s > k->rs2) {
+    const double d = k->rc2 - s;
+    S = d * d * (k->rc2 + 2.0 * s - 3.0 * k->rs2) * k->swDenomInv;
+    S1 = 6.0 * d * (k->rs2 - s) * k->swDenomInv;
+    S2 = 6.0 * (2.0 * s - k->rs2 - k->rc2) * k->swDenomInv;
+  }
+  *gA = 2.0 * (WA1 * S + WA * S1);
+  *gB = 2.0 * (WB1 * S + WB * S1);
+  *EA = WA * S;
+  *EB = WB * S;
+  *glj = A * (*gA) + B * (*gB);
+  *dglj = 2.0 * (A * (WA2 * S + 2.0 * WA1 * S1 + WA * S2) + B * (WB2 * S + 2.0 * WB1 * S1 + WB * S2));
+  const double r = sqrt(s), ri = 1.0 / r;
+  const double ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2;
+  const double h = 0.5 * k->rcinv * (3.0 - s * k->rcinv * k->rcinv);
+  const double x = k->beta * r, ex = exp(-x * x), ec = erfc(x);
+  *phf = ri - h;
+  *phs = h + (ec - 1.0) * ri;
+  *gf = -ri3 + k->rc3inv;
+  *dgf = 1.5 * ri5;
+  *gsl = -k->rc3inv - (ec - 1.0) * ri3 - k->twoBetaOverSqrtPi * ex * ri2;
+  /* d/ds of gs: (beta/sqrt(pi)) e^{-x^2} (2 beta^2 / r^2 + 3 / r^4) + 1.5 (erfc - 1) / r^5 */
+  const double b = k->beta;
+  *dgsl = 0.5 * k->twoBetaOverSqrtPi * ex * (2.0 * b * b * ri2 + 3.0 * ri2 * ri2) + 1.5 * (ec - 1.0) * ri5;
+}
+
+/* Loss of one pair (FP64). */
+static inline double pair_loss(const pair_consts* k, double s, double qq, double A, double B,
+                               double pF, double pS, double cV, double cE, double cS) {
+  double glj, dglj, gA, gB, EA, EB, gf, dgf, gsl, dgsl, phf, phs;
+  pair_second(k, s, A, B, &glj, &dglj, &gA, &gB, &EA, &EB, &gf, &dgf, &gsl, &dgsl, &phf, &phs);
+  const double Elj = A * EA + B * EB;
+  return pF * (glj + qq * gf) + pS * qq * gsl + cV * Elj + cE * qq * phf + cS * qq * phs;
+}
+
+typedef struct {
+  const double* wF; /* [3*storage] */
+  const double* wS; /* [3*storage] */
+  double cV, cE, cS;
+} oracle_cot;
+
+/* Walks the nonbonded pairs of compute c (kernel semantics: excluded pairs
+ * skipped, 1-4 pairs at full strength). onlySlot >= 0 restricts to pairs
+ * that involve that slot. Accumulates the loss and (if non-NULL) the gradients. */
+static double adjoint_compute(const oracle_system* s, const pair_consts* k, int c,
+                              const oracle_cot* cot, int onlySlot, double* gX, double* gQ,
+                              double* gA_, double* gB_) {
+  const int p1 = s->computePatch[2 * c], p2 = s->computePatch[2 * c + 1];
+  const int* P1 = s->patches + 4 * p1;
+  const int* P2 = s->patches + 4 * p2;
+  float sh[3];
+  shift_f32(s, c, sh);
+  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[1], sh[1], sh[0] * sh[0])) > 0.0f);
+  const int self = (p1 == p2) && zeroShift;
+  double shd[3];
+  for (int a = 0; a < 3; ++a)
+    shd[a] = (double)s->computeOffset[3 * c] * s->lattice[a] +
+             (double)s->computeOffset[3 * c + 1] * s->lattice[3 + a] +
+             (double)s->computeOffset[3 * c + 2] * s->lattice[6 + a];
+  const int dim = s->vdwDim;
+  double L = 0.0;
+  for (int a = 0; a < P1[0]; ++a) {
+    const int i = P1[2] + a;
+    const float* xi = s->xyzq + 4 * (size_t)i;
+    float xs[3] = {xi[0] + sh[0], xi[1] + sh[1], xi[2] + sh[2]};
+    for (int b = self ? a + 1 : 0; b < P2[0]; ++b) {
+      const int j = P2[2] + b;
+      if (onlySlot >= 0 && i != onlySlot && j != onlySlot) continue;
+      const float* xj = s->xyzq + 4 * (size_t)j;
+      const float r2f = r2_f32(xs, xj);
+      if (!(r2f < s->cutoff2f) || !(r2f < s->plcutoff2f)) continue;
+      if (!(b < P2[1] || a < P1[1])) continue;
+      if (excluded(s, i, j)) continue;
+      double d[3], uF[3], uS[3], pF = 0, pS = 0;
+      for (int q = 0; q < 3; ++q) {
+        d[q] = (double)xj[q] - ((double)xi[q] + shd[q]);
+        uF[q] = cot->wF[3 * (size_t)i + q] - cot->wF[3 * (size_t)j + q];
+        uS[q] = cot->wS[3 * (size_t)i + q] - cot->wS[3 * (size_t)j + q];
+        pF += uF[q] * d[q];
+        pS += uS[q] * d[q];
+      }
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      const int ti = s->vdwTypes[i], tj = s->vdwTypes[j];
+      const double A = s->ljA[ti * dim + tj] * s->scaling, B = s->ljB[ti * dim + tj] * s->scaling;
+      const double qi = xi[3], qj = xj[3], qq = qi * qj;
+      double glj, dglj, gA, gB, EA, EB, gf, dgf, gsl, dgsl, phf, phs;
+      pair_second(k, r2, A, B, &glj, &dglj, &gA, &gB, &EA, &EB, &gf, &dgf, &gsl, &dgsl, &phf, &phs);
+      const double g = glj + qq * gf, gs = qq * gsl;
+      L += pF * g + pS * gs + cot->cV * (A * EA + B * EB) + cot->cE * qq * phf + cot->cS * qq * phs;
+      if (gX) {
+        const double dg = dglj + qq * dgf, dgs = qq * dgsl;
+        const double radial = 2.0 * (pF * dg + pS * dgs) + cot->cV * glj + cot->cE * qq * gf +
+                              cot->cS * qq * gsl;
+        for (int q = 0; q < 3; ++q) {
+          const double v = g * uF[q] + gs * uS[q] + radial * d[q];
+          gX[3 * (size_t)j + q] += v;
+          gX[3 * (size_t)i + q] -= v;
+        }
+      }
+      if (gQ) {
+        const double dqq = pF * gf + pS * gsl + cot->cE * phf + cot->cS * phs;
+        gQ[i] += qj * dqq;
+        gQ[j] += qi * dqq;
+      }
+      if (gA_) {
+        /* d/dA and d/dB of the scaled table entries (ti, tj) */
+        gA_[ti * dim + tj] += pF * gA + cot->cV * EA;
+        gB_[ti * dim + tj] += pF * gB + cot->cV * EB;
+      }
+    }
+  }
+  return L;
+}
+
+/* Whole loss and (optionally) its FP64 gradient: gX [3*storage], gQ [storage]
+ * (w.r.t. the scaled charges in xyzq.w), gA/gB [dim*dim] (w.r.t. the scaled
+ * LJ table entries, ordered type pair (ti, tj) of i before j). */
+double oracle_adjoint(const oracle_system* s, const double* wF, const double* wS, double cV,
+                      double cE, double cS, double* gX, double* gQ, double* gA, double* gB) {
+  const pair_consts k = make_consts(s);
+  const oracle_cot cot = {wF, wS, cV, cE, cS};
+  const size_t n = (size_t)s->atomStorageSize, d2 = (size_t)s->vdwDim * s->vdwDim;
+  if (gX) memset(gX, 0, 3 * n * sizeof(double));
+  if (gQ) memset(gQ, 0, n * sizeof(double));
+  if (gA) memset(gA, 0, d2 * sizeof(double));
+  if (gB) memset(gB, 0, d2 * sizeof(double));
+  double L = 0.0;
+  int nthreads = 1;
+#ifdef _OPENMP
+  nthreads = omp_get_max_threads();
+#endif
+  double* bX = gX ? (double*)calloc(3 * n * nthreads, sizeof(double)) : NULL;
+  double* bQ = gQ ? (double*)calloc(n * nthreads, sizeof(double)) : NULL;
+  double* bA = gA ? (double*)calloc(d2 * nthreads, sizeof(double)) : NULL;
+  double* bB = gB ? (double*)calloc(d2 * nthreads, sizeof(double)) : NULL;
+#pragma omp parallel reduction(+ : L)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+#pragma omp for schedule(dynamic, 4)
+    for (int c = 0; c < s->numComputes; ++c)
+      L += adjoint_compute(s, &k, c, &cot, -1, bX ? bX + 3 * n * tid : NULL, bQ ? bQ + n * tid : NULL,
+                           bA ? bA + d2 * tid : NULL, bB ? bB + d2 * tid : NULL);
+  }
+  for (int t = 0; t < nthreads; ++t) {
+    if (gX) for (size_t q = 0; q < 3 * n; ++q) gX[q] += bX[3 * n * t + q];
+    if (gQ) for (size_t q = 0; q < n; ++q) gQ[q] += bQ[n * t + q];
+    if (gA) for (size_t q = 0; q < d2; ++q) gA[q] += bA[d2 * t + q];
+    if (gB) for (size_t q = 0; q < d2; ++q) gB[q] += bB[d2 * t + q];
+  }
+  free(bX);
+  free(bQ);
+  free(bA);
+  free(bB);
+  return L;
+}
+
+/* The part of the loss from pairs that involve slot `slot` (for central
+ * differences in that atom's position or charge). */
+double oracle_loss_local(const oracle_system* s, int slot, const double* wF, const double* wS,
+                         double cV, double cE, double cS) {
+  const pair_consts k = make_consts(s);
+  const oracle_cot cot = {wF, wS, cV, cE, cS};
+  double L = 0.0;
+  for (int c = 0; c < s->numComputes; ++c) {
+    const int p1 = s->computePatch[2 * c], p2 = s->computePatch[2 * c + 1];
+    const int* P1 = s->patches + 4 * p1;
+    const int* P2 = s->patches + 4 * p2;
+    const int in1 = slot >= P1[2] && slot < P1[2] + P1[0];
+    const int in2 = slot >= P2[2] && slot < P2[2] + P2[0];
+    if (in1 || in2) L += adjoint_compute(s, &k, c, &cot, slot, NULL, NULL, NULL, NULL);
+  }
+  return L;
+}
+
+/* Number of pairs of slot `slot` whose FP32 r^2 lies within `tol` of the
+ * cutoff^2 (central differences across such pairs are not meaningful). */
+int oracle_near_cutoff(const oracle_system* s, int slot, float tol) {
+  int n = 0;
+  for (int c = 0; c < s->numComputes; ++c) {
+    const int p1 = s->computePatch[2 * c], p2 = s->computePatch[2 * c + 1];
+    const int* P1 = s->patches + 4 * p1;
+    const int* P2 = s->patches + 4 * p2;
+    float sh[3];
+    shift_f32(s, c, sh);
+    const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[1], sh[1], sh[0] * sh[0])) > 0.0f);
+    const int self = (p1 == p2) && zeroShift;
+    for (int a = 0; a < P1[0]; ++a) {
+      const int i = P1[2] + a;
+      const float* xi = s->xyzq + 4 * (size_t)i;
+      float xs[3] = {xi[0] + sh[0], xi[1] + sh[1], xi[2] + sh[2]};
+      for (int b = self ? a + 1 : 0; b < P2[0]; ++b) {
+        const int j = P2[2] + b;
+        if (i != slot && j != slot) continue;
+        const float r2 = r2_f32(xs, s->xyzq + 4 * (size_t)j);
+        if (fabsf(r2 - s->cutoff2f) < tol) ++n;
+      }
+    }
+  }
+  return n;
+}

@@ -45,6 +45,15 @@ def lib():
                                            C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
+        L.oracle_adjoint.restype = C.c_double
+        L.oracle_adjoint.argtypes = [C.POINTER(OracleSystem), C.c_void_p, C.c_void_p, C.c_double,
+                                     C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
+        L.oracle_loss_local.restype = C.c_double
+        L.oracle_loss_local.argtypes = [C.POINTER(OracleSystem), C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_double, C.c_double]
+        L.oracle_near_cutoff.restype = C.c_int
+        L.oracle_near_cutoff.argtypes = [C.POINTER(OracleSystem), C.c_int, C.c_float]
         _lib = L
     return _lib
 
@@ -71,7 +80,7 @@ class Oracle:
         s.numPatches = packed.numPatches
         s.numComputes = packed.numComputes
         s.vdwDim = dim
-        s.xyzq = keep(packed.xyzq, np.float32)
+        s.xyzq = keep(np.array(packed.xyzq, dtype=np.float32, copy=True), np.float32)
         s.patches = keep(packed.patches, np.int32)
         s.computePatch = keep(packed.computes_patch, np.int32)
         s.computeOffset = keep(packed.computes_offset, np.float32)
@@ -136,6 +145,36 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle_nonbonded_sub failed")
         return int(self._out[21])
+
+
+    # ---- adjoint -----------------------------------------------------------
+    def adjoint(self, wF, wS, cV, cE, cS, grads=True):
+        """FP64 loss L = sum wF.F_fast + sum wS.F_slow + cV E_vdw + cE E_elec +
+        cS E_slow over the nonbonded pairs, and its gradient: (L, gX[n,3],
+        gQ[n] w.r.t. the scaled charges, gA[dim,dim], gB[dim,dim] w.r.t. the
+        scaled LJ table entries at ordered type pairs)."""
+        n = self.packed.atomStorageSize
+        dim = self.s.vdwDim
+        wF = np.ascontiguousarray(wF, dtype=np.float64)
+        wS = np.ascontiguousarray(wS, dtype=np.float64)
+        out = [np.zeros((n, 3)), np.zeros(n), np.zeros((dim, dim)), np.zeros((dim, dim))]
+        ptr = [o.ctypes.data if grads else None for o in out]
+        L = lib().oracle_adjoint(C.byref(self.s), wF.ctypes.data, wS.ctypes.data, cV, cE, cS, *ptr)
+        return (L, *out) if grads else L
+
+    def loss_local(self, slot, wF, wS, cV, cE, cS):
+        wF = np.ascontiguousarray(wF, dtype=np.float64)
+        wS = np.ascontiguousarray(wS, dtype=np.float64)
+        return lib().oracle_loss_local(C.byref(self.s), int(slot), wF.ctypes.data, wS.ctypes.data,
+                                       cV, cE, cS)
+
+    def near_cutoff(self, slot, tol):
+        return lib().oracle_near_cutoff(C.byref(self.s), int(slot), float(tol))
+
+    @property
+    def xyzq(self):
+        """The oracle's own (writable) copy of the positions and charges."""
+        return self._keep[0]
 
 
 def num_threads() -> int:
