@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kAdjThreads, 6) adjointKernel(const __grid_con
           const float dqq = fmaf(pF, gf, fmaf(pS, gs, fmaf(a.cE, phif, a.cS * phis)));
           giq = fmaf(qj, dqq, giq);
           gjq = fmaf(qi, dqq, gjq);
-          if ((ab.x != 0.0f || ab.y != 0.0f) && (mi || a.typeMask[tj])) {
+          if (mi || a.typeMask[tj]) {
             const float EA = s6 * S, EB = -s3 * S;
             atomicAdd(&s_gA[ti + tj], fmaf(pF, gA, a.cV * EA));
             atomicAdd(&s_gB[ti + tj], fmaf(pF, gB, a.cV * EB));
