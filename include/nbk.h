@@ -59,10 +59,13 @@ typedef struct { float x, y, z; } nbk_float3;
 typedef struct { float x, y, z, w; } nbk_float4;     /* CudaAtom {x,y,z,q}: src/CudaRecord.h:58-60 */
 typedef struct { int x, y; } nbk_int2;
 
-/* CudaComputeRecord, src/CudaTileListKernel.h:47-50 (20 bytes). */
+/* CudaComputeRecord, src/CudaTileListKernel.h:47-50 (24 bytes: CUDA's int2
+ * is 8-byte aligned, so the reference record ends in 4 bytes of padding and an
+ * array of them has a 24-byte stride). */
 typedef struct {
   nbk_int2 patchInd;      /* (i-patch, j-patch) indices into the patch array */
   nbk_float3 offsetXYZ;   /* i-shift in lattice units: center(pi)-center(pj)+image */
+  int pad;                /* tail padding of the reference layout; ignored */
 } nbk_compute_record;
 
 /* CudaPatchRecord with NODEGROUP_FORCE_REGISTER, src/CudaTileListKernel.h:55-63. */
@@ -73,7 +76,8 @@ typedef struct {
   int patchID;
 } nbk_patch_record;
 
-/* TileList, src/CudaTileListKernel.h:10-22 (44 bytes). */
+/* TileList, src/CudaTileListKernel.h:10-22 (48 bytes: 44 bytes of fields
+ * and, as int2 is 8-byte aligned in CUDA, 4 bytes of tail padding). */
 typedef struct {
   int iatomStart;
   int jtileStart;
@@ -82,6 +86,7 @@ typedef struct {
   nbk_int2 patchInd;
   nbk_int2 patchNumList;
   int icompute;
+  int pad;                /* tail padding of the reference layout */
 } nbk_tile_list;
 
 /* TileExcl, src/CudaTileListKernel.h:5-8: bit t of excl[lane] = 1 iff the pair

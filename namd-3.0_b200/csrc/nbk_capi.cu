@@ -16,6 +16,15 @@
 
 using namespace nbk;
 
+// Strides the reference's arrays of these records have (CUDA's int2 and
+// float4 are 8- and 16-byte aligned), so its buffers pass through unchanged.
+static_assert(sizeof(nbk_compute_record) == 24, "CudaComputeRecord is 24 bytes");
+static_assert(sizeof(nbk_tile_list) == 48, "TileList is 48 bytes");
+static_assert(sizeof(nbk_patch_record) == 16, "CudaPatchRecord (with patchID) is 16 bytes");
+static_assert(sizeof(nbk_tile_excl) == 128, "TileExcl is 128 bytes");
+static_assert(sizeof(nbk_exclusion) == 32, "CudaExclusion is 32 bytes");
+static_assert(sizeof(nbk_virial_energy) == sizeof(double) * 31, "VirialEnergy is 31 doubles");
+
 namespace {
 
 thread_local std::string g_err;
@@ -175,6 +184,8 @@ void computeConsts(nbk_context* h) {
   c.beta = (float)p.ewaldcof;
   c.beta2Pi = (float)(2.0 * p.ewaldcof / std::sqrt(M_PI));
   c.one14 = (float)(1.0 - p.scale14);
+  c.pBeta = (float)(kErfcP * p.ewaldcof);
+  c.gaussK = (float)(-p.ewaldcof * p.ewaldcof / std::log(2.0));
   c.ljDim = h->ljDim;
   c.switching = sw ? 1 : 0;
   c.hAd = 1.5 / rc;

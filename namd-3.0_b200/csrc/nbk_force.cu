@@ -21,6 +21,12 @@ constexpr int kForceWarps = 4;
 constexpr int kForceThreads = kForceWarps * kWarp;
 
 constexpr int kForceMinBlocks = 8;  // caps registers at 64 -> 32 warps per SM
+// The packed steady-state loop holds two pairs' state: up to 96 registers
+// (20 warps per SM), the two independent pairs giving each warp its own ILP.
+#ifndef NBK_STEADY_MIN_BLOCKS
+#define NBK_STEADY_MIN_BLOCKS 5
+#endif
+constexpr int kSteadyMinBlocks = NBK_STEADY_MIN_BLOCKS;
 
 // Adds a warp's fixed-point accumulators to one replica's accumulator block.
 template <bool doEnergy, bool doVirial, bool doPairlist>
@@ -51,10 +57,13 @@ __device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& a
 }
 
 template <bool doEnergy, bool doVirial, bool doSlow, bool doPairlist, bool doE64, bool doBatch>
-__global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
+__global__ void __launch_bounds__(kForceThreads,
+                                  (!doPairlist && !doE64) ? kSteadyMinBlocks : kForceMinBlocks)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
+  __shared__ float s_jx[kForceWarps][kWarp], s_jy[kForceWarps][kWarp];  // steady state: the
+  __shared__ float s_jz[kForceWarps][kWarp], s_jq[kForceWarps][kWarp];  // j tile as SoA
   __shared__ int s_type[kForceWarps][kWarp];
   __shared__ int s_jidx[kForceWarps][kWarp];
 
@@ -134,6 +143,9 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
     }
 
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fisx = 0.f, fisy = 0.f, fisz = 0.f;
+    // steady state: two partial i sums per component (packed loop below)
+    float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
+    float2 fisx2 = f2(0.f), fisy2 = f2(0.f), fisz2 = f2(0.f);
     double eV = 0.0, eE = 0.0, eS = 0.0;
     double wv[6] = {0, 0, 0, 0, 0, 0}, ws[6] = {0, 0, 0, 0, 0, 0};  // FP64 pair virials
     int activeTiles = 0;
@@ -158,21 +170,194 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
         if (lane >= nloopj) xj.x = xj.y = xj.z = 1.0e10f;
         s_jidx[wib][lane] = a.atomIndex[jstart + lane];
       }
-      s_xyzq[wib][lane] = xj;
+      if constexpr (!doPairlist && !doE64) {
+        s_jx[wib][lane] = xj.x;
+        s_jy[wib][lane] = xj.y;
+        s_jz[wib][lane] = xj.z;
+        s_jq[wib][lane] = xj.w;
+      } else {
+        s_xyzq[wib][lane] = xj;
+      }
       s_type[wib][lane] = a.vdwTypes[jstart + lane];
       __syncwarp();
 
       float fjx = 0.f, fjy = 0.f, fjz = 0.f, fjsx = 0.f, fjsy = 0.f, fjsz = 0.f;
       float eVt = 0.f, eEt = 0.f, eSt = 0.f;
       unsigned newMask = 0;
-      int tPrev = 0;
-      while (stepMask) {
-        const int t = __ffs(stepMask) - 1;
-        stepMask &= stepMask - 1;
-        // rotate the j accumulators so this lane holds those of j = (lane+t)&31
-        const int delta = t - tPrev;
-        if (delta) {
-          const int src = (lane + delta) & 31;
+      if constexpr (!doPairlist && !doE64) {
+        // Steady state: iteration k takes steps k and k+16 together through
+        // the packed FP32 math (element x = step k, element y = step k+16);
+        // iterations whose two steps are clear in every lane are skipped.
+        // i forces keep two partial sums (x, y), folded at the end of the
+        // list. j forces keep two accumulator sets: P follows step k, Q step
+        // k+16, so both rotate by the same amount; they are folded at the
+        // end of the tile.
+        float2 PQx = f2(0.f), PQy = f2(0.f), PQz = f2(0.f);     // (P, Q) fast
+        float2 PQsx = f2(0.f), PQsy = f2(0.f), PQsz = f2(0.f);  // (P, Q) slow
+        float2 eV2 = f2(0.f), eE2 = f2(0.f), eS2 = f2(0.f);
+        const float2 nXi = f2(-xi.x), nYi = f2(-xi.y), nZi = f2(-xi.z);
+        int kLast = 0;
+        unsigned mk = mask;  // bit k of the mask moved to bit 0 (and k+16 to 16)
+#pragma unroll 1
+        for (int k = 0; k < 16; ++k, mk >>= 1) {
+          if (!((stepMask >> k) & 0x10001u)) continue;  // warp-uniform
+          const int jA = (lane + k) & 31, jB = jA ^ 16;
+          const float2 X = make_float2(s_jx[wib][jA], s_jx[wib][jB]);
+          const float2 Y = make_float2(s_jy[wib][jA], s_jy[wib][jB]);
+          const float2 Z = make_float2(s_jz[wib][jA], s_jz[wib][jB]);
+          const float2 DX = add2(X, nXi), DY = add2(Y, nYi), DZ = add2(Z, nZi);
+          const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+          const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
+          const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
+          if (!__any_sync(0xffffffffu, aA || aB)) continue;
+          if (doEnergy) npair += (int)aA + (int)aB;
+          const float2 abA =
+              doBatch ? __ldg(&ljRow[ti + s_type[wib][jA]]) : s_lj[ti + s_type[wib][jA]];
+          const float2 abB =
+              doBatch ? __ldg(&ljRow[ti + s_type[wib][jB]]) : s_lj[ti + s_type[wib][jB]];
+          const float2 QQ = mul2(f2(xi.w), make_float2(s_jq[wib][jA], s_jq[wib][jB]));
+          const float2 r2s = make_float2(aA ? R2.x : c.cutoff2, aB ? R2.y : c.cutoff2);
+          const float2 qqs = make_float2(aA ? QQ.x : 0.f, aB ? QQ.y : 0.f);
+          const float2 As = make_float2(aA ? abA.x : 0.f, aB ? abB.x : 0.f);
+          const float2 nBs = make_float2(aA ? -abA.y : 0.f, aB ? -abB.y : 0.f);
+          float2 F, FS;
+          pairForce2<doEnergy, doSlow>(r2s, qqs, As, nBs, c, F, FS, eV2, eE2, eS2);
+          // i: two partial sums; inactive elements add exact zeros
+          fix2 = fma2(DX, F, fix2);
+          fiy2 = fma2(DY, F, fiy2);
+          fiz2 = fma2(DZ, F, fiz2);
+          if (doSlow) {
+            fisx2 = fma2(DX, FS, fisx2);
+            fisy2 = fma2(DY, FS, fisy2);
+            fisz2 = fma2(DZ, FS, fisz2);
+          }
+          // j: bring P to step k and Q to step k+16 (one shift for both), subtract
+          const int src = (lane + (k - kLast)) & 31;
+          kLast = k;
+          PQx = make_float2(__shfl_sync(0xffffffffu, PQx.x, src), __shfl_sync(0xffffffffu, PQx.y, src));
+          PQy = make_float2(__shfl_sync(0xffffffffu, PQy.x, src), __shfl_sync(0xffffffffu, PQy.y, src));
+          PQz = make_float2(__shfl_sync(0xffffffffu, PQz.x, src), __shfl_sync(0xffffffffu, PQz.y, src));
+          PQx = fma2(neg2(DX), F, PQx);
+          PQy = fma2(neg2(DY), F, PQy);
+          PQz = fma2(neg2(DZ), F, PQz);
+          if (doSlow) {
+            PQsx = make_float2(__shfl_sync(0xffffffffu, PQsx.x, src),
+                               __shfl_sync(0xffffffffu, PQsx.y, src));
+            PQsy = make_float2(__shfl_sync(0xffffffffu, PQsy.x, src),
+                               __shfl_sync(0xffffffffu, PQsy.y, src));
+            PQsz = make_float2(__shfl_sync(0xffffffffu, PQsz.x, src),
+                               __shfl_sync(0xffffffffu, PQsz.y, src));
+            PQsx = fma2(neg2(DX), FS, PQsx);
+            PQsy = fma2(neg2(DY), FS, PQsy);
+            PQsz = fma2(neg2(DZ), FS, PQsz);
+          }
+        }
+        // rotate P (at step kLast) and Q (at step kLast+16) back to j = lane
+        {
+          const int srcP = (lane + 32 - kLast) & 31, srcQ = (lane + 16 - kLast) & 31;
+          fjx = __shfl_sync(0xffffffffu, PQx.x, srcP) + __shfl_sync(0xffffffffu, PQx.y, srcQ);
+          fjy = __shfl_sync(0xffffffffu, PQy.x, srcP) + __shfl_sync(0xffffffffu, PQy.y, srcQ);
+          fjz = __shfl_sync(0xffffffffu, PQz.x, srcP) + __shfl_sync(0xffffffffu, PQz.y, srcQ);
+          if (doSlow) {
+            fjsx = __shfl_sync(0xffffffffu, PQsx.x, srcP) + __shfl_sync(0xffffffffu, PQsx.y, srcQ);
+            fjsy = __shfl_sync(0xffffffffu, PQsy.x, srcP) + __shfl_sync(0xffffffffu, PQsy.y, srcQ);
+            fjsz = __shfl_sync(0xffffffffu, PQsz.x, srcP) + __shfl_sync(0xffffffffu, PQsz.y, srcQ);
+          }
+        }
+        eVt = eV2.x + eV2.y;
+        eEt = eE2.x + eE2.y;
+        eSt = eS2.x + eS2.y;
+      } else {
+        int tPrev = 0;
+        while (stepMask) {
+          const int t = __ffs(stepMask) - 1;
+          stepMask &= stepMask - 1;
+          // rotate the j accumulators so this lane holds those of j = (lane+t)&31
+          const int delta = t - tPrev;
+          if (delta) {
+            const int src = (lane + delta) & 31;
+            fjx = __shfl_sync(0xffffffffu, fjx, src);
+            fjy = __shfl_sync(0xffffffffu, fjy, src);
+            fjz = __shfl_sync(0xffffffffu, fjz, src);
+            if (doSlow) {
+              fjsx = __shfl_sync(0xffffffffu, fjsx, src);
+              fjsy = __shfl_sync(0xffffffffu, fjsy, src);
+              fjsz = __shfl_sync(0xffffffffu, fjsz, src);
+            }
+          }
+          tPrev = t;
+          const int j = (lane + t) & 31;
+          const float4 xjj = s_xyzq[wib][j];
+          const float dx = __fsub_rn(xjj.x, xi.x);
+          const float dy = __fsub_rn(xjj.y, xi.y);
+          const float dz = __fsub_rn(xjj.z, xi.z);
+          const float r2 = dist2(dx, dy, dz);
+          bool active;
+          if (doPairlist) {
+            bool cand = diag ? (t > 0 && lane + t < 32) : true;
+            cand = cand && (r2 < c.plcutoff2) && (j < nfreej || lane < nfreei);
+            bool excluded = false;
+            if (cand) {
+              int diff = s_jidx[wib][j] - iIndex;
+              if (abs(diff) <= exMax) {
+                const unsigned bit = (unsigned)(diff + exBase);
+                const unsigned w = ((int)(bit >> 5) < a.numExclWords) ? __ldg(&a.exclBits[bit >> 5]) : 0u;
+                excluded = (w >> (bit & 31)) & 1u;
+              }
+              if (excluded) ++nexcl;
+              else newMask |= 1u << t;
+            }
+            active = cand && !excluded && (r2 < c.cutoff2);
+          } else {
+            active = ((mask >> t) & 1u) && (r2 < c.cutoff2);
+          }
+          if (active) {
+            if (doEnergy) ++npair;
+            const float2 ab = doBatch ? __ldg(&ljRow[ti + s_type[wib][j]]) : s_lj[ti + s_type[wib][j]];
+            float f, fs;
+            pairForce<doEnergy, doSlow>(r2, xi.w * xjj.w, ab, c, f, fs, eVt, eEt, eSt);
+            if (doE64) {
+              // electrostatic energies and the pair virials again in FP64 from
+              // FP64 geometry; the FP32 eEt/eSt are discarded in this mode
+              const double ex = (double)xjj.x - xid, ey = (double)xjj.y - yid,
+                           ez = (double)xjj.z - zid;
+              const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
+              double g, gs;
+              pairFP64<doSlow>(r2d, (double)xi.w * (double)xjj.w, (double)ab.x, (double)ab.y,
+                               a.c64, g, gs, eE, eS);
+              if (doVirial) {
+                const double d[3] = {ex, ey, ez};
+  #pragma unroll
+                for (int u = 0, q = 0; u < 3; ++u)
+  #pragma unroll
+                  for (int v = u; v < 3; ++v, ++q) {
+                    const double dd = d[u] * d[v];
+                    wv[q] = fma(-g, dd, wv[q]);
+                    if (doSlow) ws[q] = fma(-gs, dd, ws[q]);
+                  }
+              }
+            }
+            const float fx = dx * f, fy = dy * f, fz = dz * f;
+            fix += fx;
+            fiy += fy;
+            fiz += fz;
+            fjx -= fx;
+            fjy -= fy;
+            fjz -= fz;
+            if (doSlow) {
+              const float sx = dx * fs, sy = dy * fs, sz = dz * fs;
+              fisx += sx;
+              fisy += sy;
+              fisz += sz;
+              fjsx -= sx;
+              fjsy -= sy;
+              fjsz -= sz;
+            }
+          }
+        }
+        // final rotation: lane l holds the accumulators of j = l again
+        {
+          const int src = (lane + (32 - tPrev)) & 31;
           fjx = __shfl_sync(0xffffffffu, fjx, src);
           fjy = __shfl_sync(0xffffffffu, fjy, src);
           fjz = __shfl_sync(0xffffffffu, fjz, src);
@@ -181,87 +366,6 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
             fjsy = __shfl_sync(0xffffffffu, fjsy, src);
             fjsz = __shfl_sync(0xffffffffu, fjsz, src);
           }
-        }
-        tPrev = t;
-        const int j = (lane + t) & 31;
-        const float4 xjj = s_xyzq[wib][j];
-        const float dx = __fsub_rn(xjj.x, xi.x);
-        const float dy = __fsub_rn(xjj.y, xi.y);
-        const float dz = __fsub_rn(xjj.z, xi.z);
-        const float r2 = dist2(dx, dy, dz);
-        bool active;
-        if (doPairlist) {
-          bool cand = diag ? (t > 0 && lane + t < 32) : true;
-          cand = cand && (r2 < c.plcutoff2) && (j < nfreej || lane < nfreei);
-          bool excluded = false;
-          if (cand) {
-            int diff = s_jidx[wib][j] - iIndex;
-            if (abs(diff) <= exMax) {
-              const unsigned bit = (unsigned)(diff + exBase);
-              const unsigned w = ((int)(bit >> 5) < a.numExclWords) ? __ldg(&a.exclBits[bit >> 5]) : 0u;
-              excluded = (w >> (bit & 31)) & 1u;
-            }
-            if (excluded) ++nexcl;
-            else newMask |= 1u << t;
-          }
-          active = cand && !excluded && (r2 < c.cutoff2);
-        } else {
-          active = ((mask >> t) & 1u) && (r2 < c.cutoff2);
-        }
-        if (active) {
-          if (doEnergy) ++npair;
-          const float2 ab = doBatch ? __ldg(&ljRow[ti + s_type[wib][j]]) : s_lj[ti + s_type[wib][j]];
-          float f, fs;
-          pairForce<doEnergy, doSlow>(r2, xi.w * xjj.w, ab, c, f, fs, eVt, eEt, eSt);
-          if (doE64) {
-            // electrostatic energies and the pair virials again in FP64 from
-            // FP64 geometry; the FP32 eEt/eSt are discarded in this mode
-            const double ex = (double)xjj.x - xid, ey = (double)xjj.y - yid,
-                         ez = (double)xjj.z - zid;
-            const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
-            double g, gs;
-            pairFP64<doSlow>(r2d, (double)xi.w * (double)xjj.w, (double)ab.x, (double)ab.y,
-                             a.c64, g, gs, eE, eS);
-            if (doVirial) {
-              const double d[3] = {ex, ey, ez};
-#pragma unroll
-              for (int u = 0, q = 0; u < 3; ++u)
-#pragma unroll
-                for (int v = u; v < 3; ++v, ++q) {
-                  const double dd = d[u] * d[v];
-                  wv[q] = fma(-g, dd, wv[q]);
-                  if (doSlow) ws[q] = fma(-gs, dd, ws[q]);
-                }
-            }
-          }
-          const float fx = dx * f, fy = dy * f, fz = dz * f;
-          fix += fx;
-          fiy += fy;
-          fiz += fz;
-          fjx -= fx;
-          fjy -= fy;
-          fjz -= fz;
-          if (doSlow) {
-            const float sx = dx * fs, sy = dy * fs, sz = dz * fs;
-            fisx += sx;
-            fisy += sy;
-            fisz += sz;
-            fjsx -= sx;
-            fjsy -= sy;
-            fjsz -= sz;
-          }
-        }
-      }
-      // final rotation: lane l holds the accumulators of j = l again
-      {
-        const int src = (lane + (32 - tPrev)) & 31;
-        fjx = __shfl_sync(0xffffffffu, fjx, src);
-        fjy = __shfl_sync(0xffffffffu, fjy, src);
-        fjz = __shfl_sync(0xffffffffu, fjz, src);
-        if (doSlow) {
-          fjsx = __shfl_sync(0xffffffffu, fjsx, src);
-          fjsy = __shfl_sync(0xffffffffu, fjsy, src);
-          fjsz = __shfl_sync(0xffffffffu, fjsz, src);
         }
       }
       const int jatom = jstart + lane;
@@ -290,6 +394,14 @@ __global__ void __launch_bounds__(kForceThreads, kForceMinBlocks)
       }
       __syncwarp();
     }  // jt
+    if (!doPairlist && !doE64) {
+      fix = fix2.x + fix2.y;
+      fiy = fiy2.x + fiy2.y;
+      fiz = fiz2.x + fiz2.y;
+      fisx = fisx2.x + fisx2.y;
+      fisy = fisy2.x + fisy2.y;
+      fisz = fisz2.x + fisz2.y;
+    }
 
     // i forces (fixed point) and the list's shift part of the virial
     const unsigned long long qx = toFixedForce(fix), qy = toFixedForce(fiy), qz = toFixedForce(fiz);

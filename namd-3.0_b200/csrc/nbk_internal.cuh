@@ -43,6 +43,8 @@ struct NbkConst {
   float beta;         // Ewald coefficient
   float beta2Pi;      // 2 beta / sqrt(pi)
   float one14;        // 1 - scale14
+  float pBeta;        // erfcShared's p times beta (packed steady-state math)
+  float gaussK;       // -beta^2 log2(e): exp(-beta^2 r^2) = 2^(gaussK r^2)
   int ljDim;          // LJ table row length
   int switching;      // 0 when switchdist >= cutoff (plain truncated LJ)
   double hAd, hBd;    // hA, hB in FP64 (FP64 energy mode)
@@ -96,16 +98,20 @@ __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
 // were fitted by least squares on [0, 4] (fit_erfc.py; max relative error
 // 1.6e-8). `ex` is exp(-x^2), shared with the force's Gaussian term.
 constexpr float kErfcP = 4.067848869e-01f;
+constexpr float kErfcC0 = 8.043135869e-02f, kErfcC1 = -4.030445941e-01f,
+                kErfcC2 = 6.621032108e-01f, kErfcC3 = -3.509793830e-01f,
+                kErfcC4 = 3.971568035e-01f, kErfcC5 = 1.455091497e-01f,
+                kErfcC6 = 2.400594718e-01f, kErfcC7 = 2.287639988e-01f;
 __device__ __forceinline__ float erfcShared(const float x, const float ex) {
   const float t = __fdividef(1.0f, fmaf(kErfcP, x, 1.0f));
-  float q = 8.043135869e-02f;
-  q = fmaf(q, t, -4.030445941e-01f);
-  q = fmaf(q, t, 6.621032108e-01f);
-  q = fmaf(q, t, -3.509793830e-01f);
-  q = fmaf(q, t, 3.971568035e-01f);
-  q = fmaf(q, t, 1.455091497e-01f);
-  q = fmaf(q, t, 2.400594718e-01f);
-  q = fmaf(q, t, 2.287639988e-01f);
+  float q = kErfcC0;
+  q = fmaf(q, t, kErfcC1);
+  q = fmaf(q, t, kErfcC2);
+  q = fmaf(q, t, kErfcC3);
+  q = fmaf(q, t, kErfcC4);
+  q = fmaf(q, t, kErfcC5);
+  q = fmaf(q, t, kErfcC6);
+  q = fmaf(q, t, kErfcC7);
   return t * q * ex;
 }
 
@@ -156,6 +162,96 @@ __device__ __forceinline__ void pairForce(const float r2, const float qq, const 
     if (doEnergy) eSlow = fmaf(qq, fmaf(ec - 1.0f, rinv, h), eSlow);
   } else {
     fs = 0.0f;
+  }
+}
+
+// ---- two pairs at once with sm_100's packed FP32 instructions --------------
+// fma/mul/add .f32x2 issue two IEEE-rounded FP32 operations per instruction,
+// so every element below is rounded exactly as the scalar form would be;
+// only the number of issued instructions halves.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
+// PTX approximate reciprocal, base-2 exponential and reciprocal square root
+// (rcp/ex2/rsqrt.approx.ftz.f32). The inputs here are normal numbers (r^2 is
+// at least the square of the shortest pair distance, 2^(gaussK r^2) lies in
+// (2^-15, 1], 1 + p beta r lies in [1, 3]), where the ftz forms equal the
+// non-ftz ones.
+__device__ __forceinline__ float rcpApprox(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ex2Approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rsqrtApprox(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// pairForce for two pairs (x and y elements); nB = -B. An element with
+// qq = A = nB = 0 and r2 = cutoff^2 contributes exactly zero to f, fs and the
+// energies, which is how callers switch a pair off without a branch. The slow
+// term regroups the same quantities: with x = beta r, t = 1/(1 + p x) and
+// e = exp(-x^2) = 2^(gaussK r^2), erfc = t P(t) e and the force factor
+// erfc + (2 beta/sqrt(pi)) r e = (t P(t) + (2 beta/sqrt(pi)) r) e.
+template <bool doEnergy, bool doSlow>
+__device__ __forceinline__ void pairForce2(const float2 r2, const float2 qq, const float2 A,
+                                           const float2 nB, const NbkConst& c, float2& f,
+                                           float2& fs, float2& eVdw, float2& eElec,
+                                           float2& eSlow) {
+  const float2 rinv = make_float2(rsqrtApprox(r2.x), rsqrtApprox(r2.y));
+  const float2 rinv2 = mul2(rinv, rinv);
+  const float2 rinv6 = mul2(mul2(rinv2, rinv2), rinv2);
+  const float2 rinv3 = mul2(rinv, rinv2);
+  const float2 ab6 = fma2(A, rinv6, nB);
+  const float2 w = mul2(ab6, rinv6);
+  const float2 dw = mul2(fma2(A, rinv6, ab6), mul2(mul2(f2(-6.0f), rinv2), rinv6));
+  float2 s = f2(1.0f), ds = f2(0.0f);
+  if (c.switching) {
+    const float2 t2 = make_float2(fmaxf(r2.x, c.rs2), fmaxf(r2.y, c.rs2));
+    const float2 d = add2(f2(c.rc2), neg2(t2));
+    s = mul2(mul2(d, d), fma2(f2(c.lj1), t2, f2(c.lj0)));
+    ds = mul2(d, fma2(f2(c.lj2), t2, f2(c.lj3)));
+  }
+  f = fma2(w, ds, mul2(dw, s));
+  f = fma2(qq, add2(f2(c.rc3inv), neg2(rinv3)), f);
+  float2 h = f2(0.0f);
+  if (doEnergy) {
+    eVdw = fma2(w, s, eVdw);
+    h = fma2(f2(c.hB), r2, f2(c.hA));
+    eElec = fma2(qq, add2(rinv, neg2(h)), eElec);
+  }
+  if (doSlow) {
+    const float2 r = mul2(r2, rinv);
+    const float2 den = fma2(f2(c.pBeta), r, f2(1.0f));
+    const float2 t = make_float2(rcpApprox(den.x), rcpApprox(den.y));
+    const float2 g = mul2(r2, f2(c.gaussK));
+    const float2 ex = make_float2(ex2Approx(g.x), ex2Approx(g.y));
+    float2 q = f2(kErfcC0);
+    q = fma2(q, t, f2(kErfcC1));
+    q = fma2(q, t, f2(kErfcC2));
+    q = fma2(q, t, f2(kErfcC3));
+    q = fma2(q, t, f2(kErfcC4));
+    q = fma2(q, t, f2(kErfcC5));
+    q = fma2(q, t, f2(kErfcC6));
+    q = fma2(q, t, f2(kErfcC7));
+    const float2 tq = mul2(t, q);
+    const float2 corr = mul2(fma2(f2(c.beta2Pi), r, tq), ex);
+    fs = mul2(qq, fma2(add2(f2(1.0f), neg2(corr)), rinv3, f2(-c.rc3inv)));
+    if (doEnergy) {
+      const float2 ec = mul2(tq, ex);
+      eSlow = fma2(qq, fma2(add2(ec, f2(-1.0f)), rinv, h), eSlow);
+    }
+  } else {
+    fs = f2(0.0f);
   }
 }
 

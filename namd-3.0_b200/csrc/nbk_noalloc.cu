@@ -92,6 +92,8 @@ void makeConsts(const nbk_params& p, int ljDim, NbkConst& c, NbkConst64& k) {
   c.beta = (float)p.ewaldcof;
   c.beta2Pi = (float)(2.0 * p.ewaldcof / std::sqrt(M_PI));
   c.one14 = (float)(1.0 - p.scale14);
+  c.pBeta = (float)(kErfcP * p.ewaldcof);
+  c.gaussK = (float)(-p.ewaldcof * p.ewaldcof / std::log(2.0));
   c.ljDim = ljDim;
   c.switching = sw ? 1 : 0;
   c.hAd = 1.5 / rc;

@@ -726,6 +726,7 @@ NBK_API int nbk_pack(nbk_system S, double patchDim, double coulombScaling, nbk_p
               if (dz < 0 || (dz == 0 && (dy < 0 || (dy == 0 && dx < 0)))) continue;
               const int qx = (ix + dx + nx) % nx, qy = (iy + dy + ny) % ny, qz = (iz + dz + nz) % nz;
               nbk_compute_record c;
+              c.pad = 0;
               c.patchInd.x = p;
               c.patchInd.y = qx + nx * (qy + ny * qz);
               // center(p) - center(q) + image, in lattice units == -d / n

@@ -34,7 +34,7 @@ class Int2(C.Structure):
 
 
 class ComputeRecord(C.Structure):
-    _fields_ = [("patchInd", Int2), ("offsetXYZ", Float3)]
+    _fields_ = [("patchInd", Int2), ("offsetXYZ", Float3), ("pad", C.c_int)]
 
 
 class PatchRecord(C.Structure):
@@ -45,7 +45,7 @@ class PatchRecord(C.Structure):
 class TileList(C.Structure):
     _fields_ = [("iatomStart", C.c_int), ("jtileStart", C.c_int), ("jtileEnd", C.c_int),
                 ("offsetXYZ", Float3), ("patchInd", Int2), ("patchNumList", Int2),
-                ("icompute", C.c_int)]
+                ("icompute", C.c_int), ("pad", C.c_int)]
 
 
 class TileListStat(C.Structure):
@@ -300,9 +300,10 @@ class Packed:
         self.exclIndexMaxDiff = _arr(v.exclIndexMaxDiff, 2 * n, np.int32).reshape(n, 2)
         self.exclusionBits = _arr(v.exclusionBits, v.numExclusionWords, np.uint32)
         self.patches = _arr(v.patches, 4 * v.numPatches, np.int32).reshape(-1, 4)
-        comp = _arr(v.computes, 5 * v.numComputes, np.int32).reshape(-1, 5)
+        comp = _arr(v.computes, 6 * v.numComputes, np.int32).reshape(-1, 6)
+        self.computes = comp                                 # raw nbk_compute_record words
         self.computes_patch = comp[:, :2]
-        self.computes_offset = comp[:, 2:].view(np.float32)
+        self.computes_offset = comp[:, 2:5].view(np.float32)
         self.slotOfAtom = _arr(v.slotOfAtom, v.natoms, np.int32)
         self.patchCenter = _arr(v.patchCenter, 3 * v.numPatches, np.float64).reshape(-1, 3)
         ex_dt = np.dtype([("i", np.int32), ("j", np.int32), ("ti", np.int32), ("tj", np.int32),
@@ -547,7 +548,7 @@ class Nonbonded:
         L = dev_lib()
         _dcheck(L.nbk_export_tile_lists(self._h, C.byref(nl), C.byref(nj), None, None, None,
                                         stream), "nbk_export_tile_lists")
-        tl = np.zeros((max(nl.value, 1), 11), dtype=np.int32)
+        tl = np.zeros((max(nl.value, 1), 12), dtype=np.int32)
         ja = np.zeros(max(nj.value, 1), dtype=np.int32)
         ex = np.zeros((max(nj.value, 1), 32), dtype=np.uint32)
         _dcheck(L.nbk_export_tile_lists(self._h, C.byref(nl), C.byref(nj), tl.ctypes.data,

@@ -40,3 +40,18 @@ def test_create_without_gpu_fails_cleanly():
     lj = (1, [1.0], [1.0], [1.0], [1.0])
     with pytest.raises(nbk.NbkError):
         nbk.Nonbonded(nbk.NonbondedParams(), lj)
+
+
+def test_record_layouts_match_reference():
+    """Array strides of the records the boundary shares with the reference.
+    CUDA's int2 is 8-byte aligned, so CudaComputeRecord {int2, float3} is 24
+    bytes and TileList 48 (src/CudaTileListKernel.h:10-22,47-50); a caller's
+    arrays of the reference structs must pass through unchanged."""
+    assert C.sizeof(nbk.ComputeRecord) == 24
+    assert C.sizeof(nbk.TileList) == 48
+    assert C.sizeof(nbk.PatchRecord) == 16
+    assert C.sizeof(nbk.TileExcl) == 128
+    assert C.sizeof(nbk.Exclusion) == 32
+    assert C.sizeof(nbk.VirialEnergy) == 31 * 8
+    assert nbk.ComputeRecord.offsetXYZ.offset == 8
+    assert nbk.TileList.patchInd.offset == 24 and nbk.TileList.icompute.offset == 40
