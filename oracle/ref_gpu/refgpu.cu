@@ -309,6 +309,7 @@ struct RefGpu {
   CudaComputeNonbondedKernel* nb = nullptr;
   DeviceCUDA* dc = nullptr;
   cudaStream_t stream = nullptr;
+  bool ownStream = true;
   CudaNBConstants c;
   float cutoff2 = 0.f, plcutoff2 = 0.f;
   int doTable = 1;
@@ -494,6 +495,23 @@ int refgpu_sync(void* hp) {
 }
 
 void* refgpu_stream(void* hp) { return ((RefGpu*)hp)->stream; }
+
+// Runs this instance on a caller's stream from now on (NULL: back to its
+// own). Several instances on one stream evaluate one after another.
+int refgpu_set_stream(void* hp, void* stream) {
+  RefGpu* h = (RefGpu*)hp;
+  return guarded(h, [&] {
+    ck(cudaStreamSynchronize(h->stream), "set_stream sync");
+    if (stream) {
+      if (h->ownStream) ck(cudaStreamDestroy(h->stream), "own stream destroy");
+      h->stream = (cudaStream_t)stream;
+      h->ownStream = false;
+    } else if (!h->ownStream) {
+      ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "stream");
+      h->ownStream = true;
+    }
+  });
+}
 void* refgpu_device_xyzq(void* hp) { return ((RefGpu*)hp)->tl->get_xyzq(); }
 void* refgpu_device_forces(void* hp, int slow) {
   RefGpu* h = (RefGpu*)hp;
@@ -566,7 +584,7 @@ int refgpu_destroy(void* hp) {
     if (h->d_forces) cudaFree(h->d_forces);
     if (h->d_forcesSlow) cudaFree(h->d_forcesSlow);
     if (h->d_ve) cudaFree(h->d_ve);
-    cudaStreamDestroy(h->stream);
+    if (h->ownStream) cudaStreamDestroy(h->stream);
     delete h->dc;
   });
   deviceCUDA = nullptr;

@@ -34,6 +34,7 @@ def lib() -> C.CDLL:
         L.refgpu_sync.argtypes = [vp]
         L.refgpu_stream.argtypes = [vp]
         L.refgpu_stream.restype = vp
+        L.refgpu_set_stream.argtypes = [vp, vp]
         L.refgpu_device_xyzq.argtypes = [vp]
         L.refgpu_device_xyzq.restype = vp
         L.refgpu_results.argtypes = [vp, vp, vp, vp]
@@ -73,6 +74,10 @@ class RefGpu:
     @property
     def stream_ptr(self) -> int:
         return lib().refgpu_stream(self._h) or 0
+
+    def set_stream(self, stream_ptr):
+        """Evaluate on a caller's CUDA stream (an int handle; 0: own stream)."""
+        _check(lib().refgpu_set_stream(self._h, stream_ptr or None), "refgpu_set_stream")
 
     def setup(self, packed):
         self.n = packed.atomStorageSize

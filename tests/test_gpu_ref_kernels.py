@@ -12,8 +12,9 @@ by oracle/ref_gpu/Makefile).
   per-pair error near 1e-5 that the cancelling electrostatic sums amplify;
   the product's error on the same system is asserted to be smaller.
 - Timing: the reference's plain GPU path and the product on the 92,224-atom
-  mixed system, steady-state and pairlist steps, CUDA events on each path's
-  stream.
+  mixed system, steady-state and pairlist steps, and on 64 independent
+  replicas (the reference one instance per replica, the product batched),
+  CUDA events on each path's stream.
 """
 import json
 
@@ -215,3 +216,68 @@ def test_ref_kernel_launches_small(mixed):
     run.build()
     for flags in (ALL | nbk.NBK_PAIRLIST, ALL, ALL):
         run.eval(flags)
+
+
+def test_ref_plain_batch64_timing():
+    """64 independent replicas (log-uniform 2,000-40,000 atoms, 0.1 atoms/A^3,
+    own seeds; the benchmark's replica set): the reference plain GPU path,
+    one reference instance and one launch sequence per replica back to back
+    on one stream, against the product's batched handle (all replicas in one
+    launch sequence), steady-state energy + virial + slow evaluations with
+    positions resident on the device."""
+    import torch
+    rng = np.random.default_rng(20261203)
+    sizes = np.exp(rng.uniform(np.log(2000), np.log(40000), 64)).astype(int)
+    systems = [nbk.System(nbk.NBK_SYS_MIXED, 5000 + r, int(n), 0.3) for r, n in enumerate(sizes)]
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+    refs = []
+    for sy in systems:
+        pk = nbk.Packed(sy)
+        ref = _ref_run(sy, pk, 1)
+        ref.set_stream(sp)
+        ref.eval(1, 1, 1, 1, np.ascontiguousarray(pk.xyzq))
+        refs.append(ref)
+    K = 20
+
+    def timed(fn, k):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(2):
+            fn()
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / k
+
+    def ref_round():
+        for ref in refs:
+            ref.eval(0, 1, 1, 1, None)
+    ref_ms = timed(ref_round, K)
+
+    many = nbk.Packed.many(systems)
+    nb = nbk.Nonbonded(PARAMS, systems[0].lj_table(), 0)
+    nb.setup(many, stream=sp)
+    nb.set_replicas(many, stream=sp)
+    n = many.atomStorageSize
+    with torch.cuda.stream(stream):
+        x = torch.from_numpy(many.xyzq.copy()).cuda()
+        dF = torch.zeros((n, 4), device="cuda")
+        dS = torch.zeros((n, 4), device="cuda")
+        dVE = torch.zeros((64, 32), dtype=torch.float64, device="cuda")
+    FL = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
+    nb.build_tile_lists(many, xyzq=x, stream=sp)
+    nb.force(many, FL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=sp)
+
+    def batch_round():
+        nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=sp)
+        nb.virial_energy_batch_to(dVE.data_ptr(), True, stream=sp)
+    batch_ms = timed(batch_round, K)
+    out = {"replicas": 64, "atoms": int(sizes.sum()), "ref_plain_ms_per_round": round(ref_ms, 4),
+           "product_batched_ms_per_round": round(batch_ms, 4),
+           "ref_plain_replica_evals_per_s": round(64e3 / ref_ms, 1),
+           "product_batched_replica_evals_per_s": round(64e3 / batch_ms, 1),
+           "speedup": round(ref_ms / batch_ms, 3)}
+    print("batch64 plain-path timing " + json.dumps(out))
+    assert ref_ms > 0 and batch_ms > 0
