@@ -188,6 +188,7 @@ void computeConsts(nbk_context* h) {
   c.gaussK = (float)(-p.ewaldcof * p.ewaldcof / std::log(2.0));
   c.ljDim = h->ljDim;
   c.switching = sw ? 1 : 0;
+  c.s0 = sw ? 0.0f : 1.0f;
   c.hAd = 1.5 / rc;
   c.hBd = -0.5 / (rc * rc2);
   c.betad = p.ewaldcof;

@@ -62,8 +62,9 @@ __global__ void __launch_bounds__(kForceThreads,
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
-  __shared__ float s_jx[kForceWarps][kWarp], s_jy[kForceWarps][kWarp];  // steady state: the
-  __shared__ float s_jz[kForceWarps][kWarp], s_jq[kForceWarps][kWarp];  // j tile as SoA
+  // steady state: the j tile as five rows (x, y, z, q, type bits) so that one
+  // address per j serves all of its loads
+  __shared__ float s_jt[kForceWarps][5][kWarp];
   __shared__ int s_type[kForceWarps][kWarp];
   __shared__ int s_jidx[kForceWarps][kWarp];
 
@@ -171,10 +172,11 @@ __global__ void __launch_bounds__(kForceThreads,
         s_jidx[wib][lane] = a.atomIndex[jstart + lane];
       }
       if constexpr (!doPairlist && !doE64) {
-        s_jx[wib][lane] = xj.x;
-        s_jy[wib][lane] = xj.y;
-        s_jz[wib][lane] = xj.z;
-        s_jq[wib][lane] = xj.w;
+        s_jt[wib][0][lane] = xj.x;
+        s_jt[wib][1][lane] = xj.y;
+        s_jt[wib][2][lane] = xj.z;
+        s_jt[wib][3][lane] = xj.w;
+        s_jt[wib][4][lane] = __int_as_float(a.vdwTypes[jstart + lane]);
       } else {
         s_xyzq[wib][lane] = xj;
       }
@@ -198,24 +200,25 @@ __global__ void __launch_bounds__(kForceThreads,
         const float2 nXi = f2(-xi.x), nYi = f2(-xi.y), nZi = f2(-xi.z);
         int kLast = 0;
         unsigned mk = mask;  // bit k of the mask moved to bit 0 (and k+16 to 16)
-#pragma unroll 1
+#pragma unroll 2
         for (int k = 0; k < 16; ++k, mk >>= 1) {
           if (!((stepMask >> k) & 0x10001u)) continue;  // warp-uniform
           const int jA = (lane + k) & 31, jB = jA ^ 16;
-          const float2 X = make_float2(s_jx[wib][jA], s_jx[wib][jB]);
-          const float2 Y = make_float2(s_jy[wib][jA], s_jy[wib][jB]);
-          const float2 Z = make_float2(s_jz[wib][jA], s_jz[wib][jB]);
+          const float* pA = &s_jt[wib][0][jA];
+          const float* pB = &s_jt[wib][0][jB];
+          const float2 X = make_float2(pA[0], pB[0]);
+          const float2 Y = make_float2(pA[32], pB[32]);
+          const float2 Z = make_float2(pA[64], pB[64]);
           const float2 DX = add2(X, nXi), DY = add2(Y, nYi), DZ = add2(Z, nZi);
           const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
           const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
           const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
           if (!__any_sync(0xffffffffu, aA || aB)) continue;
           if (doEnergy) npair += (int)aA + (int)aB;
-          const float2 abA =
-              doBatch ? __ldg(&ljRow[ti + s_type[wib][jA]]) : s_lj[ti + s_type[wib][jA]];
-          const float2 abB =
-              doBatch ? __ldg(&ljRow[ti + s_type[wib][jB]]) : s_lj[ti + s_type[wib][jB]];
-          const float2 QQ = mul2(f2(xi.w), make_float2(s_jq[wib][jA], s_jq[wib][jB]));
+          const int tyA = __float_as_int(pA[128]), tyB = __float_as_int(pB[128]);
+          const float2 abA = doBatch ? __ldg(&ljRow[ti + tyA]) : s_lj[ti + tyA];
+          const float2 abB = doBatch ? __ldg(&ljRow[ti + tyB]) : s_lj[ti + tyB];
+          const float2 QQ = mul2(f2(xi.w), make_float2(pA[96], pB[96]));
           const float2 r2s = make_float2(aA ? R2.x : c.cutoff2, aB ? R2.y : c.cutoff2);
           const float2 qqs = make_float2(aA ? QQ.x : 0.f, aB ? QQ.y : 0.f);
           const float2 As = make_float2(aA ? abA.x : 0.f, aB ? abB.x : 0.f);

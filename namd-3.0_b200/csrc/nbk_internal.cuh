@@ -45,6 +45,7 @@ struct NbkConst {
   float one14;        // 1 - scale14
   float pBeta;        // erfcShared's p times beta (packed steady-state math)
   float gaussK;       // -beta^2 log2(e): exp(-beta^2 r^2) = 2^(gaussK r^2)
+  float s0;           // 0 with switching, 1 without (packed math: S = d^2 P + s0)
   int ljDim;          // LJ table row length
   int switching;      // 0 when switchdist >= cutoff (plain truncated LJ)
   double hAd, hBd;    // hA, hB in FP64 (FP64 energy mode)
@@ -214,13 +215,12 @@ __device__ __forceinline__ void pairForce2(const float2 r2, const float2 qq, con
   const float2 ab6 = fma2(A, rinv6, nB);
   const float2 w = mul2(ab6, rinv6);
   const float2 dw = mul2(fma2(A, rinv6, ab6), mul2(mul2(f2(-6.0f), rinv2), rinv6));
-  float2 s = f2(1.0f), ds = f2(0.0f);
-  if (c.switching) {
-    const float2 t2 = make_float2(fmaxf(r2.x, c.rs2), fmaxf(r2.y, c.rs2));
-    const float2 d = add2(f2(c.rc2), neg2(t2));
-    s = mul2(mul2(d, d), fma2(f2(c.lj1), t2, f2(c.lj0)));
-    ds = mul2(d, fma2(f2(c.lj2), t2, f2(c.lj3)));
-  }
+  // switch without a branch: without switching rs2 = rc2 and lj0..lj3 = 0,
+  // so d = 0 for every pair inside the cutoff and S = s0 = 1, dS = 0
+  const float2 t2 = make_float2(fmaxf(r2.x, c.rs2), fmaxf(r2.y, c.rs2));
+  const float2 d = add2(f2(c.rc2), neg2(t2));
+  const float2 s = fma2(mul2(d, d), fma2(f2(c.lj1), t2, f2(c.lj0)), f2(c.s0));
+  const float2 ds = mul2(d, fma2(f2(c.lj2), t2, f2(c.lj3)));
   f = fma2(w, ds, mul2(dw, s));
   f = fma2(qq, add2(f2(c.rc3inv), neg2(rinv3)), f);
   float2 h = f2(0.0f);

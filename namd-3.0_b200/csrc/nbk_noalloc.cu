@@ -96,6 +96,7 @@ void makeConsts(const nbk_params& p, int ljDim, NbkConst& c, NbkConst64& k) {
   c.gaussK = (float)(-p.ewaldcof * p.ewaldcof / std::log(2.0));
   c.ljDim = ljDim;
   c.switching = sw ? 1 : 0;
+  c.s0 = sw ? 0.0f : 1.0f;
   c.hAd = 1.5 / rc;
   c.hBd = -0.5 / (rc * rc2);
   c.betad = p.ewaldcof;
