@@ -106,7 +106,7 @@ struct nbk_context {
   DBuf<nbk_tile_list> lists2;
   DBuf<int> jatom2;
   DBuf<nbk_tile_excl> excl2;
-  DBuf<int> counters;  // [0] lists kept, [1] j tiles kept, [2] force-kernel work counter
+  DBuf<int> counters;  // [0] lists kept, [1] j tiles kept, [2] force / [3] refine work counters
   bool built = false;     // tile lists built (sparse)
   bool refined = false;   // compacted lists valid
   float3 lata{}, latb{}, latc{};
@@ -584,29 +584,22 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     a.repLat = h->repLat.p;
     a.repLJ = h->repLJ.p;
   }
-  NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
-  if (pairlist) {
-    a.lists = h->lists1.p;
-    a.numListsDev = nullptr;
-    a.numListsHost = h->numLists;
-    a.tileJatomStart = h->jatom1.p;
-    a.tileExcls = h->excl1.p;
-    a.jtileActive = h->jtileActive.p;
-    a.listActive = h->listActive.p;
-    a.patchPairs = h->patchPairs.p;
-  } else {
-    a.lists = h->lists2.p;
-    a.numListsDev = h->counters.p;
-    a.numListsHost = 0;
-    a.tileJatomStart = h->jatom2.p;
-    a.tileExcls = h->excl2.p;
-  }
   NBK_CUDA(timedEvent(h, true, st), "timing event");
-  NBK_CUDA(launchForce(a, flags, h->numSM, st), "force kernel");
-  NBK_CUDA(timedEvent(h, false, st), "timing event");
-  h->launches += 1;
   if (pairlist) {
-    // compaction of the refined lists (reSortTileLists), on the device
+    // refinement of the culled lists (the pairlist pass), then their
+    // compaction (reSortTileLists), both on the device
+    ForceArgs r = a;
+    r.lists = h->lists1.p;
+    r.numListsDev = nullptr;
+    r.numListsHost = h->numLists;
+    r.tileJatomStart = h->jatom1.p;
+    r.tileExcls = h->excl1.p;
+    r.jtileActive = h->jtileActive.p;
+    r.listActive = h->listActive.p;
+    r.patchPairs = h->patchPairs.p;
+    r.workCounter = h->counters.p + 3;
+    NBK_CUDA(cudaMemsetAsync(h->counters.p + 3, 0, sizeof(int), st), "nbk_nonbonded_force");
+    NBK_CUDA(launchRefine(r, h->numSM, st), "pairlist refinement");
     const int nl = std::max(h->numLists, 1), nj = std::max(h->jcap, 1);
     NBK_CUDA(h->lists2.ensure(nl), "nbk_nonbonded_force");
     NBK_CUDA(h->jatom2.ensure(nj), "nbk_nonbonded_force");
@@ -615,9 +608,18 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     NBK_CUDA(launchCompact(h->numLists, h->lists1.p, h->listActive.p, h->jtileActive.p, h->jatom1.p,
                            h->excl1.p, h->lists2.p, h->jatom2.p, h->excl2.p, h->counters.p,
                            h->numSM, st), "tile-list compaction");
-    h->launches += 1;
+    h->launches += 2;
     h->refined = true;
   }
+  a.lists = h->lists2.p;
+  a.numListsDev = h->counters.p;
+  a.numListsHost = 0;
+  a.tileJatomStart = h->jatom2.p;
+  a.tileExcls = h->excl2.p;
+  NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
+  NBK_CUDA(launchForce(a, flags, h->numSM, st), "force kernel");
+  NBK_CUDA(timedEvent(h, false, st), "timing event");
+  h->launches += 1;
   if ((flags & NBK_CORRECTIONS) && (h->numMod || h->numExc)) {
     if (h->maxTupleSlot >= n)
       return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: a correction tuple names a slot beyond atomStorageSize");

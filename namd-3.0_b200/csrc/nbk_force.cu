@@ -6,8 +6,10 @@
 //   - j forces ride in registers and rotate one lane per step with a shuffle
 //     (lane l works on j = (l+t) & 31 at step t), so the inner loop touches
 //     shared memory only for the broadcast-free j coordinate load;
-//   - in steady state, steps whose bit is clear in every lane's mask are
-//     skipped warp-uniformly (the rotation jumps by the step distance);
+//   - steps whose bit is clear in every lane's mask are skipped warp-uniformly
+//     (the rotation jumps by the step distance);
+//   - the lists it reads are already refined (TileExcl masks from
+//     refineKernel); a pairlist step refines, compacts, then runs this kernel;
 //   - per-tile FP32 partial forces are folded into 64-bit fixed point with
 //     integer atomics, so the summed forces do not depend on the order in
 //     which lists run; energies and virials are folded into fixed point per
@@ -20,8 +22,8 @@ namespace nbk {
 constexpr int kForceWarps = 4;
 constexpr int kForceThreads = kForceWarps * kWarp;
 
-constexpr int kForceMinBlocks = 8;  // caps registers at 64 -> 32 warps per SM
-// The packed steady-state loop holds two pairs' state: up to 96 registers
+// The packed FP32 loop holds two pairs' state (and the FP64 energy mode its
+// FP64 pair virials): up to 96 registers
 // (20 warps per SM), the two independent pairs giving each warp its own ILP.
 #ifndef NBK_STEADY_MIN_BLOCKS
 #define NBK_STEADY_MIN_BLOCKS 5
@@ -29,22 +31,16 @@ constexpr int kForceMinBlocks = 8;  // caps registers at 64 -> 32 warps per SM
 constexpr int kSteadyMinBlocks = NBK_STEADY_MIN_BLOCKS;
 
 // Adds a warp's fixed-point accumulators to one replica's accumulator block.
-template <bool doEnergy, bool doVirial, bool doPairlist>
+template <bool doEnergy, bool doVirial>
 __device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& accE0,
                                           long long& accE1, long long& accE2, long long& accVir,
-                                          int& nexcl, int& npair) {
+                                          int& npair) {
   if (doVirial && lane < 18 && accVir != 0)
     atomicAddFixed(&acc[kAccVir + lane], (unsigned long long)accVir);
   if (doEnergy && lane == 0) {
     if (accE0) atomicAddFixed(&acc[kAccEVdw], (unsigned long long)accE0);
     if (accE1) atomicAddFixed(&acc[kAccEElec], (unsigned long long)accE1);
     if (accE2) atomicAddFixed(&acc[kAccESlow], (unsigned long long)accE2);
-  }
-  if (doPairlist) {
-    int s = nexcl;
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0 && s) atomicAddFixed(&acc[kAccNumExcl], (unsigned long long)s);
   }
   if (doEnergy) {
     int s = npair;
@@ -53,20 +49,18 @@ __device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& a
     if (lane == 0 && s) atomicAddFixed(&acc[kAccNumPairs], (unsigned long long)s);
   }
   accE0 = accE1 = accE2 = accVir = 0;
-  nexcl = npair = 0;
+  npair = 0;
 }
 
-template <bool doEnergy, bool doVirial, bool doSlow, bool doPairlist, bool doE64, bool doBatch>
-__global__ void __launch_bounds__(kForceThreads,
-                                  (!doPairlist && !doE64) ? kSteadyMinBlocks : kForceMinBlocks)
+template <bool doEnergy, bool doVirial, bool doSlow, bool doE64, bool doBatch>
+__global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
-  // steady state: the j tile as five rows (x, y, z, q, type bits) so that one
+  // packed loop: the j tile as five rows (x, y, z, q, type bits) so that one
   // address per j serves all of its loads
   __shared__ float s_jt[kForceWarps][5][kWarp];
   __shared__ int s_type[kForceWarps][kWarp];
-  __shared__ int s_jidx[kForceWarps][kWarp];
 
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -82,7 +76,6 @@ __global__ void __launch_bounds__(kForceThreads,
   // per-warp fixed-point accumulators: lane k < 9 owns virial[k], 9 <= k < 18
   // owns virialSlow[k-9]; lane 0 also owns the three energies.
   long long accE0 = 0, accE1 = 0, accE2 = 0, accVir = 0;
-  int nexcl = 0;
   int npair = 0;  // interacting pairs seen by this lane (energy evaluations)
   int curRep = 0;  // replica whose accumulators the warp is holding
 
@@ -100,8 +93,8 @@ __global__ void __launch_bounds__(kForceThreads,
     if (doBatch) {
       const int rep = __ldg(&a.compRep[tl.icompute]);
       if (rep != curRep) {
-        flushWarp<doEnergy, doVirial, doPairlist>(a.acc + (size_t)curRep * kAccCount, lane, accE0,
-                                                  accE1, accE2, accVir, nexcl, npair);
+        flushWarp<doEnergy, doVirial>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1,
+                                      accE2, accVir, npair);
         curRep = rep;
       }
       la = a.repLat[3 * rep];
@@ -112,7 +105,6 @@ __global__ void __launch_bounds__(kForceThreads,
     const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
     const float3 sh = shiftOf(off, la, lb, lc);
     const bool zeroShift = !(dist2(sh.x, sh.y, sh.z) > 0.0f);
-    const bool selfCompute = (tl.patchInd.x == tl.patchInd.y) && zeroShift;
 
     const int iatom = tl.iatomStart + lane;
     float4 xi = a.xyzq[iatom];
@@ -129,49 +121,20 @@ __global__ void __launch_bounds__(kForceThreads,
     xi.z = __fadd_rn(xi.z, sh.z);
     const int ti = a.vdwTypes[iatom] * dim;
 
-    int nfreei = 32, jatomSize = 0, jatomFreeSize = 0, iIndex = 0, exBase = 0, exMax = -1;
-    if (doPairlist) {
-      const PatchPair pp = a.patchPairs[L];
-      const int nloopi = min(pp.iatomSize - tl.iatomStart, 32);
-      nfreei = max(pp.iatomFreeSize - tl.iatomStart, 0);
-      jatomSize = pp.jatomSize;
-      jatomFreeSize = pp.jatomFreeSize;
-      if (lane >= nloopi) xi.x = xi.y = xi.z = -1.0e10f;
-      iIndex = a.atomIndex[iatom];
-      const int2 em = a.exclIndexMaxDiff[iatom];
-      exBase = em.x;
-      exMax = em.y;
-    }
-
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fisx = 0.f, fisy = 0.f, fisz = 0.f;
     // steady state: two partial i sums per component (packed loop below)
     float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
     float2 fisx2 = f2(0.f), fisy2 = f2(0.f), fisz2 = f2(0.f);
     double eV = 0.0, eE = 0.0, eS = 0.0;
     double wv[6] = {0, 0, 0, 0, 0, 0}, ws[6] = {0, 0, 0, 0, 0, 0};  // FP64 pair virials
-    int activeTiles = 0;
 
     for (int jt = tl.jtileStart; jt <= tl.jtileEnd; ++jt) {
       const int jstart = a.tileJatomStart[jt];
-      unsigned mask = 0;
-      unsigned stepMask;
-      if (!doPairlist) {
-        mask = a.tileExcls[jt].excl[lane];
-        stepMask = __reduce_or_sync(0xffffffffu, mask);
-        if (stepMask == 0) continue;
-      } else {
-        stepMask = 0xffffffffu;
-      }
-      const bool diag = selfCompute && (jstart == tl.iatomStart);
-      float4 xj = a.xyzq[jstart + lane];
-      int nfreej = 32;
-      if (doPairlist) {
-        const int nloopj = min(jatomSize - jstart, 32);
-        nfreej = max(jatomFreeSize - jstart, 0);
-        if (lane >= nloopj) xj.x = xj.y = xj.z = 1.0e10f;
-        s_jidx[wib][lane] = a.atomIndex[jstart + lane];
-      }
-      if constexpr (!doPairlist && !doE64) {
+      const unsigned mask = a.tileExcls[jt].excl[lane];
+      unsigned stepMask = __reduce_or_sync(0xffffffffu, mask);
+      if (stepMask == 0) continue;
+      const float4 xj = a.xyzq[jstart + lane];
+      if constexpr (!doE64) {
         s_jt[wib][0][lane] = xj.x;
         s_jt[wib][1][lane] = xj.y;
         s_jt[wib][2][lane] = xj.z;
@@ -185,9 +148,8 @@ __global__ void __launch_bounds__(kForceThreads,
 
       float fjx = 0.f, fjy = 0.f, fjz = 0.f, fjsx = 0.f, fjsy = 0.f, fjsz = 0.f;
       float eVt = 0.f, eEt = 0.f, eSt = 0.f;
-      unsigned newMask = 0;
-      if constexpr (!doPairlist && !doE64) {
-        // Steady state: iteration k takes steps k and k+16 together through
+      if constexpr (!doE64) {
+        // Iteration k takes steps k and k+16 together through
         // the packed FP32 math (element x = step k, element y = step k+16);
         // iterations whose two steps are clear in every lane are skipped.
         // i forces keep two partial sums (x, y), folded at the end of the
@@ -295,26 +257,7 @@ __global__ void __launch_bounds__(kForceThreads,
           const float dy = __fsub_rn(xjj.y, xi.y);
           const float dz = __fsub_rn(xjj.z, xi.z);
           const float r2 = dist2(dx, dy, dz);
-          bool active;
-          if (doPairlist) {
-            bool cand = diag ? (t > 0 && lane + t < 32) : true;
-            cand = cand && (r2 < c.plcutoff2) && (j < nfreej || lane < nfreei);
-            bool excluded = false;
-            if (cand) {
-              int diff = s_jidx[wib][j] - iIndex;
-              if (abs(diff) <= exMax) {
-                const unsigned bit = (unsigned)(diff + exBase);
-                const unsigned w = ((int)(bit >> 5) < a.numExclWords) ? __ldg(&a.exclBits[bit >> 5]) : 0u;
-                excluded = (w >> (bit & 31)) & 1u;
-              }
-              if (excluded) ++nexcl;
-              else newMask |= 1u << t;
-            }
-            active = cand && !excluded && (r2 < c.cutoff2);
-          } else {
-            active = ((mask >> t) & 1u) && (r2 < c.cutoff2);
-          }
-          if (active) {
+          if (((mask >> t) & 1u) && (r2 < c.cutoff2)) {
             if (doEnergy) ++npair;
             const float2 ab = doBatch ? __ldg(&ljRow[ti + s_type[wib][j]]) : s_lj[ti + s_type[wib][j]];
             float f, fs;
@@ -389,15 +332,9 @@ __global__ void __launch_bounds__(kForceThreads,
           if (doSlow) eS += (double)eSt;
         }
       }
-      if (doPairlist) {
-        a.tileExcls[jt].excl[lane] = newMask;
-        const bool any = __any_sync(0xffffffffu, newMask != 0);
-        if (lane == 0) a.jtileActive[jt] = any ? 1 : 0;
-        activeTiles += any ? 1 : 0;
-      }
       __syncwarp();
     }  // jt
-    if (!doPairlist && !doE64) {
+    if (!doE64) {
       fix = fix2.x + fix2.y;
       fiy = fiy2.x + fiy2.y;
       fiz = fiz2.x + fiz2.y;
@@ -470,19 +407,18 @@ __global__ void __launch_bounds__(kForceThreads,
         accE2 += toFixedEnergy(sS);
       }
     }
-    if (doPairlist && lane == 0) a.listActive[L] = activeTiles;
   }  // lists
 
   // per-warp flush of the fixed-point accumulators (no block barrier, so a
   // warp that runs out of lists retires at once)
-  flushWarp<doEnergy, doVirial, doPairlist>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1,
-                                            accE2, accVir, nexcl, npair);
+  flushWarp<doEnergy, doVirial>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1, accE2,
+                                accVir, npair);
 }
 
-template <bool E, bool V, bool S, bool P, bool D, bool B>
+template <bool E, bool V, bool S, bool D, bool B>
 static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
   const size_t shmem = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
-  auto k = forceKernel<E, V, S, P, D, B>;
+  auto k = forceKernel<E, V, S, D, B>;
   static int cachedDim = -1, cachedBlocks = 0;
   if (cachedDim != a.c.ljDim) {
     if (shmem > 48 * 1024) {
@@ -502,54 +438,33 @@ static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st) {
   const bool E = flags & NBK_ENERGY;
   const bool B = a.compRep != nullptr;
-  const int idx = (B ? 32 : 0) | (E ? 16 : 0) | ((flags & NBK_VIRIAL) ? 8 : 0) |
-                  ((flags & NBK_SLOW) ? 4 : 0) | ((flags & NBK_PAIRLIST) ? 2 : 0) |
-                  ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
+  const int idx = (B ? 16 : 0) | (E ? 8 : 0) | ((flags & NBK_VIRIAL) ? 4 : 0) |
+                  ((flags & NBK_SLOW) ? 2 : 0) | ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
   switch (idx) {
-#define NBK_CASE(i, e, v, s, p, d, b) \
-  case i:                             \
-    return launchT<e, v, s, p, d, b>(a, numSM, st);
-    NBK_CASE(0, false, false, false, false, false, false)
-    NBK_CASE(2, false, false, false, true, false, false)
-    NBK_CASE(4, false, false, true, false, false, false)
-    NBK_CASE(6, false, false, true, true, false, false)
-    NBK_CASE(8, false, true, false, false, false, false)
-    NBK_CASE(10, false, true, false, true, false, false)
-    NBK_CASE(12, false, true, true, false, false, false)
-    NBK_CASE(14, false, true, true, true, false, false)
-    NBK_CASE(16, true, false, false, false, false, false)
-    NBK_CASE(17, true, false, false, false, true, false)
-    NBK_CASE(18, true, false, false, true, false, false)
-    NBK_CASE(19, true, false, false, true, true, false)
-    NBK_CASE(20, true, false, true, false, false, false)
-    NBK_CASE(21, true, false, true, false, true, false)
-    NBK_CASE(22, true, false, true, true, false, false)
-    NBK_CASE(23, true, false, true, true, true, false)
-    NBK_CASE(24, true, true, false, false, false, false)
-    NBK_CASE(25, true, true, false, false, true, false)
-    NBK_CASE(26, true, true, false, true, false, false)
-    NBK_CASE(27, true, true, false, true, true, false)
-    NBK_CASE(28, true, true, true, false, false, false)
-    NBK_CASE(29, true, true, true, false, true, false)
-    NBK_CASE(30, true, true, true, true, false, false)
-    NBK_CASE(31, true, true, true, true, true, false)
+#define NBK_CASE(i, e, v, s, d, b) \
+  case i:                          \
+    return launchT<e, v, s, d, b>(a, numSM, st);
+    NBK_CASE(0, false, false, false, false, false)
+    NBK_CASE(2, false, false, true, false, false)
+    NBK_CASE(4, false, true, false, false, false)
+    NBK_CASE(6, false, true, true, false, false)
+    NBK_CASE(8, true, false, false, false, false)
+    NBK_CASE(9, true, false, false, true, false)
+    NBK_CASE(10, true, false, true, false, false)
+    NBK_CASE(11, true, false, true, true, false)
+    NBK_CASE(12, true, true, false, false, false)
+    NBK_CASE(13, true, true, false, true, false)
+    NBK_CASE(14, true, true, true, false, false)
+    NBK_CASE(15, true, true, true, true, false)
     // batched replicas (FP32 energy mode)
-    NBK_CASE(32, false, false, false, false, false, true)
-    NBK_CASE(34, false, false, false, true, false, true)
-    NBK_CASE(36, false, false, true, false, false, true)
-    NBK_CASE(38, false, false, true, true, false, true)
-    NBK_CASE(40, false, true, false, false, false, true)
-    NBK_CASE(42, false, true, false, true, false, true)
-    NBK_CASE(44, false, true, true, false, false, true)
-    NBK_CASE(46, false, true, true, true, false, true)
-    NBK_CASE(48, true, false, false, false, false, true)
-    NBK_CASE(50, true, false, false, true, false, true)
-    NBK_CASE(52, true, false, true, false, false, true)
-    NBK_CASE(54, true, false, true, true, false, true)
-    NBK_CASE(56, true, true, false, false, false, true)
-    NBK_CASE(58, true, true, false, true, false, true)
-    NBK_CASE(60, true, true, true, false, false, true)
-    NBK_CASE(62, true, true, true, true, false, true)
+    NBK_CASE(16, false, false, false, false, true)
+    NBK_CASE(18, false, false, true, false, true)
+    NBK_CASE(20, false, true, false, false, true)
+    NBK_CASE(22, false, true, true, false, true)
+    NBK_CASE(24, true, false, false, false, true)
+    NBK_CASE(26, true, false, true, false, true)
+    NBK_CASE(28, true, true, false, false, true)
+    NBK_CASE(30, true, true, true, false, true)
 #undef NBK_CASE
   }
   return cudaErrorInvalidValue;

@@ -325,10 +325,10 @@ struct ForceArgs {
   const int* numListsDev;      // device count (compacted lists) or NULL
   int numListsHost;            // used when numListsDev == NULL
   const int* tileJatomStart;
-  nbk_tile_excl* tileExcls;    // read (steady) / written (pairlist)
-  int* jtileActive;            // pairlist: written
-  int* listActive;             // pairlist: number of active j-tiles per list
-  const PatchPair* patchPairs; // pairlist
+  nbk_tile_excl* tileExcls;    // read by the force kernel, written by refineKernel
+  int* jtileActive;            // refineKernel: written
+  int* listActive;             // refineKernel: number of active j-tiles per list
+  const PatchPair* patchPairs; // refineKernel
   const float4* xyzq;
   const int* vdwTypes;
   const int* atomIndex;

@@ -8,6 +8,9 @@
 namespace nbk {
 
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st);
+// Pairlist refinement of the culled lists a.lists[0, a.numListsHost): writes
+// a.tileExcls, a.jtileActive, a.listActive and the excluded-pair counts.
+cudaError_t launchRefine(const ForceArgs& a, int numSM, cudaStream_t st);
 
 cudaError_t launchBBoxes(int numTiles, const float4* xyzq, BBox* bb, cudaStream_t st);
 

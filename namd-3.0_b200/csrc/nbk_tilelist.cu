@@ -161,6 +161,113 @@ __global__ void compactKernel(int numLists, const nbk_tile_list* __restrict__ sr
   }
 }
 
+// Pairlist refinement without force math: for every j tile of every culled
+// list, bit t of TileExcl.excl[lane] is set when the pair (i = iatomStart +
+// lane, j = jatomStart + ((lane + t) & 31)) lies within the pairlist cutoff
+// (FP32 r^2 with the shift and operand order of shiftOf / dist2), is not a
+// padding pair, is not the diagonal or lower triangle of a self tile and is
+// not a full exclusion (the pairlist pass of nonbondedForceKernel,
+// src/CudaComputeNonbondedKernel.cu:1202-1249,1424-1443). Writes the masks
+// in place, jtileActive / listActive for the compaction and the per-replica
+// count of excluded pairs within the pairlist cutoff. One warp per list,
+// lists handed out from a.workCounter.
+__global__ void __launch_bounds__(128) refineKernel(const __grid_constant__ ForceArgs a) {
+  __shared__ float4 s_xyzq[4][32];
+  __shared__ int s_jidx[4][32];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  const float plc2 = a.c.plcutoff2;
+  int nexcl = 0, curRep = 0;
+  for (;;) {
+    int L = 0;
+    if (lane == 0) L = atomicAdd(a.workCounter, 1);
+    L = __shfl_sync(0xffffffffu, L, 0);
+    if (L >= a.numListsHost) break;
+    const nbk_tile_list tl = a.lists[L];
+    if (tl.jtileEnd < tl.jtileStart) continue;  // warp-uniform
+    float3 la = a.lata, lb = a.latb, lc = a.latc;
+    if (a.compRep) {
+      const int rep = __ldg(&a.compRep[tl.icompute]);
+      if (rep != curRep) {
+        const int s = __reduce_add_sync(0xffffffffu, nexcl);
+        if (lane == 0 && s) atomicAddFixed(&a.acc[(size_t)curRep * kAccCount + kAccNumExcl], (unsigned long long)s);
+        nexcl = 0;
+        curRep = rep;
+      }
+      la = a.repLat[3 * rep];
+      lb = a.repLat[3 * rep + 1];
+      lc = a.repLat[3 * rep + 2];
+    }
+    const float3 sh = shiftOf(make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z), la, lb, lc);
+    const bool zeroShift = !(dist2(sh.x, sh.y, sh.z) > 0.0f);
+    const bool selfCompute = (tl.patchInd.x == tl.patchInd.y) && zeroShift;
+    const int iatom = tl.iatomStart + lane;
+    const PatchPair pp = a.patchPairs[L];
+    const int nloopi = min(pp.iatomSize - tl.iatomStart, 32);
+    const int nfreei = max(pp.iatomFreeSize - tl.iatomStart, 0);
+    float4 xi = a.xyzq[iatom];
+    xi.x = __fadd_rn(xi.x, sh.x);
+    xi.y = __fadd_rn(xi.y, sh.y);
+    xi.z = __fadd_rn(xi.z, sh.z);
+    if (lane >= nloopi) xi.x = xi.y = xi.z = -1.0e10f;
+    const int iIndex = a.atomIndex[iatom];
+    const int2 em = a.exclIndexMaxDiff[iatom];
+    int activeTiles = 0;
+    for (int jt = tl.jtileStart; jt <= tl.jtileEnd; ++jt) {
+      const int jstart = a.tileJatomStart[jt];
+      const bool diag = selfCompute && (jstart == tl.iatomStart);
+      const int nloopj = min(pp.jatomSize - jstart, 32);
+      const int nfreej = max(pp.jatomFreeSize - jstart, 0);
+      float4 xj = a.xyzq[jstart + lane];
+      if (lane >= nloopj) xj.x = xj.y = xj.z = 1.0e10f;
+      s_xyzq[wib][lane] = xj;
+      s_jidx[wib][lane] = a.atomIndex[jstart + lane];
+      __syncwarp();
+      unsigned m = 0;
+#pragma unroll 4
+      for (int t = 0; t < 32; ++t) {
+        const int j = (lane + t) & 31;
+        const float4 x = s_xyzq[wib][j];
+        const float r2 = dist2(__fsub_rn(x.x, xi.x), __fsub_rn(x.y, xi.y), __fsub_rn(x.z, xi.z));
+        const bool cand = (diag ? (t > 0 && lane + t < 32) : true) && (r2 < plc2) &&
+                          (j < nfreej || lane < nfreei);
+        if (cand) {
+          bool excluded = false;
+          const int diff = s_jidx[wib][j] - iIndex;
+          if (abs(diff) <= em.y) {
+            const unsigned bit = (unsigned)(diff + em.x);
+            const unsigned w = ((int)(bit >> 5) < a.numExclWords) ? __ldg(&a.exclBits[bit >> 5]) : 0u;
+            excluded = (w >> (bit & 31)) & 1u;
+          }
+          if (excluded) ++nexcl;
+          else m |= 1u << t;
+        }
+      }
+      a.tileExcls[jt].excl[lane] = m;
+      const bool any = __any_sync(0xffffffffu, m != 0);
+      if (lane == 0) a.jtileActive[jt] = any ? 1 : 0;
+      activeTiles += any ? 1 : 0;
+      __syncwarp();
+    }
+    if (lane == 0) a.listActive[L] = activeTiles;
+  }
+  const int s = __reduce_add_sync(0xffffffffu, nexcl);
+  if (lane == 0 && s) atomicAddFixed(&a.acc[(size_t)curRep * kAccCount + kAccNumExcl], (unsigned long long)s);
+}
+
+cudaError_t launchRefine(const ForceArgs& a, int numSM, cudaStream_t st) {
+  if (a.numListsHost <= 0) return cudaSuccess;
+  static int cachedBlocks = 0;
+  if (!cachedBlocks) {
+    int nb = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, refineKernel, 128, 0);
+    if (e != cudaSuccess) return e;
+    cachedBlocks = nb > 0 ? nb : 1;
+  }
+  refineKernel<<<numSM * cachedBlocks, 128, 0, st>>>(a);
+  return cudaGetLastError();
+}
+
 cudaError_t launchBBoxes(int numTiles, const float4* xyzq, BBox* bb, cudaStream_t st) {
   if (numTiles <= 0) return cudaSuccess;
   const int threads = 256;
