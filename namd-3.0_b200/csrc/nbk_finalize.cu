@@ -263,10 +263,13 @@ cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st
 // (reduceNonbondedVirialKernel, :1649-1763), folded into fixed point per atom.
 // Each warp owns a contiguous slot range so that, with batched replicas, its
 // slots belong to one replica except at boundaries.
-__global__ void finalizeKernel(int n, const long long* __restrict__ F, int stride,
-                               const float4* __restrict__ xyzq, float4* __restrict__ outF,
-                               float4* __restrict__ outS, int doSlow, int doVirial,
-                               long long* __restrict__ accBase, const int* __restrict__ slotRep) {
+constexpr int kFinalizeThreads = 256;
+
+__global__ void __launch_bounds__(kFinalizeThreads)
+    finalizeKernel(int n, const long long* __restrict__ F, int stride,
+                   const float4* __restrict__ xyzq, float4* __restrict__ outF,
+                   float4* __restrict__ outS, int doSlow, int doVirial,
+                   long long* __restrict__ accBase, const int* __restrict__ slotRep) {
   long long v[18] = {};
   const int lane = threadIdx.x & 31;
   const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
@@ -316,16 +319,40 @@ __global__ void finalizeKernel(int n, const long long* __restrict__ F, int strid
     }
   }
   if (!doVirial) return;
+  // Reduce the warp, then the block, before touching the 18 accumulator
+  // words: every block adds each word once (per-warp adds only where a block
+  // spans two replicas), which keeps same-address atomics off the critical path.
+  __shared__ long long s_v[kFinalizeThreads / 32][18];
+  __shared__ int s_rep[kFinalizeThreads / 32];
+  const int wib = threadIdx.x >> 5;
   const int rep0 = __shfl_sync(0xffffffffu, curRep, 0);
   const bool uniform = __all_sync(0xffffffffu, curRep == rep0);
 #pragma unroll
   for (int p = 0; p < 18; ++p) {
     if (p >= 9 && !doSlow) break;
     if (uniform) {
-      const long long s = warpSumLL(v[p]);
-      if (lane == 0 && s != 0) atomicAddFixed(&accBase[(size_t)rep0 * kAccCount + kAccVir + p], (unsigned long long)s);
-    } else if (v[p] != 0) {
-      atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
+      const long long sw = warpSumLL(v[p]);
+      if (lane == 0) s_v[wib][p] = sw;
+    } else {
+      if (v[p] != 0) atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
+      if (lane == 0) s_v[wib][p] = 0;
+    }
+  }
+  if (lane == 0) s_rep[wib] = uniform ? rep0 : -1;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  if (threadIdx.x < 18 && (threadIdx.x < 9 || doSlow)) {
+    const int p = threadIdx.x;
+    bool same = true;
+    for (int w = 1; w < nw; ++w) same = same && (s_rep[w] == s_rep[0] || s_rep[w] < 0);
+    if (same && s_rep[0] >= 0) {
+      long long sb = 0;
+      for (int w = 0; w < nw; ++w) sb += s_v[w][p];
+      if (sb != 0) atomicAddFixed(&accBase[(size_t)s_rep[0] * kAccCount + kAccVir + p], (unsigned long long)sb);
+    } else {
+      for (int w = 0; w < nw; ++w)
+        if (s_rep[w] >= 0 && s_v[w][p] != 0)
+          atomicAddFixed(&accBase[(size_t)s_rep[w] * kAccCount + kAccVir + p], (unsigned long long)s_v[w][p]);
     }
   }
 }
@@ -336,8 +363,8 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
   if (n <= 0) return cudaSuccess;
   const bool V = flags & NBK_VIRIAL;
   if (!V && !outF && !outS) return cudaSuccess;
-  const int threads = 256;
-  const int blocks = min((n + threads - 1) / threads, numSM * 4);
+  const int threads = kFinalizeThreads;
+  const int blocks = min((n + threads - 1) / threads, numSM);
   // the FP64 energy/virial mode accumulates complete pair virials instead
   const bool atomVirial = V && !((flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64));
   if (!atomVirial && !outF && !outS) return cudaSuccess;
