@@ -43,6 +43,20 @@ WORKLOAD = ("mixed-92224: 92,224 atoms (30% random-walk chains + TIP3P-like wate
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "force_kernel_mixed92k.json")
 
 
+def use_large_system():
+    """Switches the single-system workload to the precision study's system:
+    1,066,628 atoms, 25% random-walk chains, cube at 0.1 atoms/A^3 (220 A),
+    20-frame trajectory (the same step protocol as the 92k workload)."""
+    global METRIC, NATOMS, BOX, FRAC, NFRAMES, WORKLOAD, PROFILE_TRAFFIC
+    METRIC = "nonbonded pairs/s at 1.07M atoms (force err<=1e-5)"
+    NATOMS, BOX, FRAC, NFRAMES = 1066628, None, 0.25, 20
+    WORKLOAD = ("large-1066628: 1,066,628 atoms (25% random-walk chains + TIP3P-like water), "
+                "cube 220.1 A, cutoff 12 / switch 10 / pairlist 13.5 A, ewaldcof 0.2579; "
+                "energy+virial+slow every eval; lists rebuilt every 10 evals; "
+                "20-frame trajectory with N(0,0.02 A) steps")
+    PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "force_kernel_large1m.json")
+
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -513,14 +527,18 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--workload", choices=["mixed92k", "batch64", "adjoint24k"], default="mixed92k",
-                    help="batch64: 64-replica batched launch vs one launch per replica")
+    ap.add_argument("--workload", choices=["mixed92k", "batch64", "adjoint24k", "large1m"],
+                    default="mixed92k",
+                    help="batch64: 64-replica batched launch vs one launch per replica; "
+                         "large1m: the 1,066,628-atom system of the precision study")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "large1m":
+        use_large_system()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
