@@ -234,11 +234,13 @@ def run_gpu(args, rank, world, local_rank):
     for k in range(NFRAMES):
         step(k)
         pairs_of[k] = nb.pair_count(st)
+    # launch shape of the force kernel: chosen once by the autotuner, untimed
+    shape = nb.autotune(FL, iterations=5, stream=st)
     for k in range(args.warmup):
         step(k)
     torch.cuda.synchronize(dev)
     log(f"[rank {rank}] setup {time.perf_counter() - t_setup:.1f}s, storage {n}, "
-        f"pairs/eval {pairs_of.mean():.4g}")
+        f"pairs/eval {pairs_of.mean():.4g}, launch shape {shape}")
 
     dist = None
     if world > 1:
@@ -347,6 +349,7 @@ def run_gpu(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "atoms": NATOMS, "atom_slots": n,
                        "pairs_per_eval": float(pairs_of.mean()), "rebuild_every": REBUILD,
+                       "launch_shape": shape,
                        "l2": "flushed (512 MB write) between timed steps, outside the events",
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "evals_per_s": args.steps / (total_ms * 1e-3) * world,
@@ -393,6 +396,7 @@ def run_batch(args, rank, world, local_rank):
         nb.force(many, FL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
         nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
         pairs = int(nb.pair_counts(st).sum())
+        shape = nb.autotune(FL, iterations=3, stream=st)
         for _ in range(args.warmup):
             nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
             nb.virial_energy_batch_to(dVE.data_ptr(), True, stream=st)
@@ -427,6 +431,7 @@ def run_batch(args, rank, world, local_rank):
             ver = torch.zeros(32, dtype=torch.float64, device=dev)
             h.build_tile_lists(pk, xyzq=xr, stream=st)
             h.force(pk, FL | nbk.NBK_PAIRLIST, xyzq=xr, d_forces=fr, d_forcesSlow=sr, stream=st)
+            h.autotune(FL, iterations=3, stream=st)
             plain.append((h, pk, xr, fr, sr, ver))
         ksteps = max(3, min(args.steps, 200))
         pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
@@ -452,6 +457,7 @@ def run_batch(args, rank, world, local_rank):
         "config": {"workload": "batch64: 64 mixed replicas, log-uniform 2,000-40,000 atoms, "
                                "0.1 atoms/A^3, own seeds; steady-state force+energy+virial+slow",
                    "atoms": int(sizes.sum()), "pairs_per_batch_eval": pairs,
+                   "launch_shape": shape,
                    "l2": "flushed between timed steps"},
         "pairs_per_s": pairs * args.steps / (batched_ms * 1e-3),
         "plain_one_launch_per_replica": {"value": plainv, "unit": "replica-evals/s",

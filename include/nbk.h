@@ -324,6 +324,33 @@ NBK_API long long nbk_launch_count(nbk_handle h);
  * register-resident FMA loop over all SMs (synchronises; ~50 ms). */
 NBK_API int nbk_measure_fp32_peak(int deviceID, double* tflops);
 
+/* Autotuner of the force kernel's launch shape (no counterpart in the
+ * reference, whose launch shape is fixed: NONBONDKERNEL_NUM_WARP warps per
+ * block, src/CudaComputeNonbondedKernel.cu:32,2151-2152). Times every shape on
+ * the handle's current refined lists, positions and lattice (those of the last
+ * nbk_nonbonded_force call, which must still be valid) with `iterations`
+ * launches each, and keeps the fastest for this flag combination (energy,
+ * virial, slow, FP64 energy mode; batched or not): CTAs per SM 4, 5 or 6 (the
+ * register cap: 128, 96 or 80 registers) times 1, 2 or 4 warps per tile list
+ * (a list's j tiles split into contiguous parts handed out separately; the
+ * FP64 energy mode always uses one). The choice changes no result: per-tile
+ * FP32 partials are folded into integer fixed point at the end of every j
+ * tile and all further sums are integer. Synchronises the stream; overwrites the handle's force
+ * and energy accumulators, so call it before an evaluation, not between an
+ * evaluation and its nbk_reduce_virial_energy. Untuned handles use 5 CTAs per
+ * SM and one warp per list; the tuner keeps that default unless another shape
+ * is at least 3% faster, since shapes are timed back to back on a warm L2. */
+NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* stream);
+
+/* The launch shape in use for a flag combination and the time per force
+ * launch measured by nbk_autotune (0 before tuning). */
+NBK_API int nbk_get_tuning(nbk_handle h, unsigned flags, int* minBlocksPerSM, int* listSplit,
+                           float* ms);
+
+/* Pins the launch shape for a flag combination without timing (CTAs per SM 4,
+ * 5 or 6; 1, 2 or 4 warps per tile list). */
+NBK_API int nbk_set_tuning(nbk_handle h, unsigned flags, int minBlocksPerSM, int listSplit);
+
 #ifdef __cplusplus
 }
 #endif

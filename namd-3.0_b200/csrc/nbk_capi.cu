@@ -130,6 +130,16 @@ struct nbk_context {
   DBuf<long long> adjGrad;
   DBuf<int> typeMask;
   int adjStride = 0;
+  // launch shape of the force kernel per flag combination (tuneKey): CTAs per
+  // SM and log2 of the work items per list; set by nbk_autotune
+  int tuneMinBlocks[32];
+  int tuneSplitLog2[32];
+  float tuneMs[32];
+  float lastCutoff2 = 0.f;
+  // [numComputes][6] i-force sums per compute (shift virial): the tail of the
+  // force buffer, cleared by the same memset
+  long long* compF = nullptr;
+  int compFComputes = 0;
   // measurement
   long long launches = 0;
   bool timing = false;
@@ -208,6 +218,51 @@ void computeConsts(nbk_context* h) {
   k.switching = sw ? 1 : 0;
 }
 
+// Index of a flag combination in the tuning tables (the force kernel variant).
+int tuneKey(const nbk_context* h, unsigned flags) {
+  const bool E = flags & NBK_ENERGY;
+  return (h->nrep > 0 ? 16 : 0) | (E ? 8 : 0) | ((flags & NBK_VIRIAL) ? 4 : 0) |
+         ((flags & NBK_SLOW) ? 2 : 0) | ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
+}
+
+// Force-kernel arguments for the handle's compacted lists, positions, lattice,
+// constants and replicas.
+ForceArgs refinedForceArgs(nbk_context* h, float cutoff2) {
+  ForceArgs a{};
+  a.xyzq = h->xyzq;
+  a.vdwTypes = h->vdwTypes.p;
+  a.atomIndex = h->atomIndex.p;
+  a.exclIndexMaxDiff = h->exclIndexMaxDiff.p;
+  a.exclBits = h->exclBits.p;
+  a.numExclWords = h->numExclWords;
+  a.ljTable = h->ljTable.p;
+  a.lata = h->lata;
+  a.latb = h->latb;
+  a.latc = h->latc;
+  a.c = h->c;
+  a.c.cutoff2 = cutoff2;
+  a.force = h->force.p;
+  a.stride = h->atomStorageSize;
+  a.acc = h->acc.p;
+  a.workCounter = h->counters.p + 2;
+  a.c64 = h->c64;
+  if (h->nrep > 0) {
+    a.compRep = h->compRep.p;
+    a.repLat = h->repLat.p;
+    a.repLJ = h->repLJ.p;
+  }
+  a.lists = h->lists2.p;
+  a.numListsDev = h->counters.p;
+  a.numListsHost = 0;
+  a.tileJatomStart = h->jatom2.p;
+  a.tileExcls = h->excl2.p;
+  a.compF = h->compF;
+  return a;
+}
+
+// The FP64 energy mode keeps its per-pair FP64 sums per list: one warp per list.
+bool fp64Energy(unsigned flags) { return (flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64); }
+
 int checkHandle(nbk_handle h, const char* fn) {
   if (!h) return setErr(NBK_ERR_ARG, std::string(fn) + ": NULL handle");
   cudaError_t e = cudaSetDevice(h->device);
@@ -275,6 +330,11 @@ NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
   h->prm.ljA = h->prm.ljB = h->prm.ljA14 = h->prm.ljB14 = nullptr;
   h->ljDim = p->vdwTableDim;
   computeConsts(h);
+  for (int k = 0; k < 32; ++k) {
+    h->tuneMinBlocks[k] = 5;
+    h->tuneSplitLog2[k] = 0;
+    h->tuneMs[k] = 0.f;
+  }
   // LJ tables (CudaNonbondedTables::buildVdwCoefTable, src/CudaNonbondedTables.C:110-148)
   const int dim = h->ljDim;
   std::vector<float2> t(dim * dim), te(dim * dim);
@@ -547,11 +607,15 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   rc = bindPositions(h, xyzq, xyzqOnDevice, atomStorageSize, st, "nbk_nonbonded_force");
   if (rc) return rc;
   const int n = atomStorageSize;
-  if (h->forceStride != n) {
-    NBK_CUDA(h->force.ensure(6 * (size_t)n), "nbk_nonbonded_force");
+  if (h->forceStride != n || h->compFComputes != h->numComputes) {
+    NBK_CUDA(h->force.ensure(6 * ((size_t)n + (size_t)h->numComputes)), "nbk_nonbonded_force");
     h->forceStride = n;
+    h->compFComputes = h->numComputes;
   }
-  NBK_CUDA(cudaMemsetAsync(h->force.p, 0, sizeof(long long) * 6 * (size_t)n, st), "nbk_nonbonded_force");
+  h->compF = h->force.p + 6 * (size_t)n;
+  NBK_CUDA(cudaMemsetAsync(h->force.p, 0,
+                           sizeof(long long) * 6 * ((size_t)n + (size_t)h->numComputes), st),
+           "nbk_nonbonded_force");
   if (h->nrep > 0 && (flags & NBK_ENERGY_FP64) && (flags & NBK_ENERGY))
     return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: NBK_ENERGY_FP64 is not available with replicas");
   const int accBlocks = h->nrep > 0 ? h->nrep : 1;
@@ -561,29 +625,11 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   h->latb = f3(latb);
   h->latc = f3(latc);
 
-  ForceArgs a{};
-  a.xyzq = h->xyzq;
-  a.vdwTypes = h->vdwTypes.p;
-  a.atomIndex = h->atomIndex.p;
-  a.exclIndexMaxDiff = h->exclIndexMaxDiff.p;
-  a.exclBits = h->exclBits.p;
-  a.numExclWords = h->numExclWords;
-  a.ljTable = h->ljTable.p;
-  a.lata = h->lata;
-  a.latb = h->latb;
-  a.latc = h->latc;
-  a.c = h->c;
-  a.c.cutoff2 = cutoff2;
-  a.force = h->force.p;
-  a.stride = n;
-  a.acc = h->acc.p;
-  a.workCounter = h->counters.p + 2;
-  a.c64 = h->c64;
-  if (h->nrep > 0) {
-    a.compRep = h->compRep.p;
-    a.repLat = h->repLat.p;
-    a.repLJ = h->repLJ.p;
-  }
+  h->lastCutoff2 = cutoff2;
+  const bool shiftVirial = (flags & NBK_VIRIAL) && !fp64Energy(flags);
+  ForceArgs a = refinedForceArgs(h, cutoff2);
+  const int key = tuneKey(h, flags);
+  a.splitLog2 = fp64Energy(flags) ? 0 : h->tuneSplitLog2[key];
   NBK_CUDA(timedEvent(h, true, st), "timing event");
   if (pairlist) {
     // refinement of the culled lists (the pairlist pass), then their
@@ -611,13 +657,12 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     h->launches += 2;
     h->refined = true;
   }
+  // compacted lists (the pairlist block above may have grown these buffers)
   a.lists = h->lists2.p;
-  a.numListsDev = h->counters.p;
-  a.numListsHost = 0;
   a.tileJatomStart = h->jatom2.p;
   a.tileExcls = h->excl2.p;
   NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
-  NBK_CUDA(launchForce(a, flags, h->numSM, st), "force kernel");
+  NBK_CUDA(launchForce(a, flags, h->tuneMinBlocks[key], h->numSM, st), "force kernel");
   NBK_CUDA(timedEvent(h, false, st), "timing event");
   h->launches += 1;
   if ((flags & NBK_CORRECTIONS) && (h->numMod || h->numExc)) {
@@ -647,9 +692,21 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     NBK_CUDA(launchCorrections(ca, flags, st), "exclusion corrections");
     h->launches += 1;
   }
+  ShiftVirialArgs sv{};
+  if (shiftVirial) {
+    sv.numComputes = h->numComputes;
+    sv.compF = h->compF;
+    sv.computes = h->computes.p;
+    sv.lata = h->lata;
+    sv.latb = h->latb;
+    sv.latc = h->latc;
+    sv.compRep = h->nrep ? h->compRep.p : nullptr;
+    sv.repLat = h->nrep ? h->repLat.p : nullptr;
+  }
   NBK_CUDA(launchFinalizeForces(n, h->force.p, n, h->xyzq, reinterpret_cast<float4*>(d_forces),
                                 (flags & NBK_SLOW) ? reinterpret_cast<float4*>(d_forcesSlow) : nullptr,
-                                flags, h->acc.p, h->numSM, st, h->nrep ? h->slotRep.p : nullptr),
+                                flags, h->acc.p, h->numSM, st, h->nrep ? h->slotRep.p : nullptr,
+                                &sv),
            "force finalize");
   if ((flags & NBK_VIRIAL) || d_forces || d_forcesSlow) h->launches += 1;
   if (d_forcesFixed)
@@ -972,5 +1029,102 @@ extern "C" NBK_API int nbk_measure_fp32_peak(int deviceID, double* tflops) {
   cudaEventDestroy(e1);
   cudaFree(out);
   *tflops = best;
+  return NBK_OK;
+}
+
+NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* stream) {
+  int rc = checkHandle(h, "nbk_autotune");
+  if (rc) return rc;
+  if (!h->refined)
+    return setErr(NBK_ERR_STATE, "nbk_autotune: needs refined tile lists (an NBK_PAIRLIST evaluation) first");
+  if (flags & ~63u) return setErr(NBK_ERR_ARG, "nbk_autotune: unknown flag bits");
+  if (h->nrep > 0 && (flags & NBK_ENERGY_FP64) && (flags & NBK_ENERGY))
+    return setErr(NBK_ERR_ARG, "nbk_autotune: NBK_ENERGY_FP64 is not available with replicas");
+  if (iterations < 1) iterations = 1;
+  cudaStream_t st = (cudaStream_t)stream;
+  const unsigned kflags = flags & ~(unsigned)(NBK_PAIRLIST | NBK_CORRECTIONS);
+  const int key = tuneKey(h, kflags);
+  const int n = h->atomStorageSize;
+  const int accBlocks = h->nrep > 0 ? h->nrep : 1;
+  ForceArgs a = refinedForceArgs(h, h->lastCutoff2);
+  const int maxSplitLog2 = fp64Energy(kflags) ? 0 : 2;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  NBK_CUDA(cudaEventCreate(&e0), "nbk_autotune");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return setErr(NBK_ERR_CUDA, "nbk_autotune: event");
+  }
+  // shapes are timed back to back on a warm L2; another shape replaces the
+  // default (5 CTAs per SM, one warp per list) only when it is at least 3%
+  // faster, so that timing noise does not pick a shape that loses in use
+  float bestMs = 1e30f, defaultMs = 1e30f;
+  int bestB = 5, bestS = 0;
+  cudaError_t err = cudaSuccess;
+  const int shapes[3] = {4, 5, 6};
+  for (int bi = 0; bi < 3 && err == cudaSuccess; ++bi) {
+    for (int sl = 0; sl <= maxSplitLog2 && err == cudaSuccess; ++sl) {
+      a.splitLog2 = sl;
+      for (int it = -1; it < iterations && err == cudaSuccess; ++it) {  // it = -1: untimed
+        if (it == 0) err = cudaEventRecord(e0, st);
+        if (err == cudaSuccess) err = cudaMemsetAsync(h->force.p, 0, sizeof(long long) * 6 * (size_t)n, st);
+        if (err == cudaSuccess)
+          err = cudaMemsetAsync(h->acc.p, 0, sizeof(long long) * kAccCount * (size_t)accBlocks, st);
+        if (err == cudaSuccess) err = cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st);
+        if (err == cudaSuccess) err = launchForce(a, kflags, shapes[bi], h->numSM, st);
+        h->launches += 1;
+      }
+      if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+      if (err == cudaSuccess) {
+        const float t = ms / iterations;
+        if (shapes[bi] == 5 && sl == 0) defaultMs = t;
+        if (t < bestMs) {
+          bestMs = t;
+          bestB = shapes[bi];
+          bestS = sl;
+        }
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return setErr(NBK_ERR_CUDA, std::string("nbk_autotune: ") + cudaGetErrorString(err));
+  if (!(bestMs < 0.97f * defaultMs)) {
+    bestB = 5;
+    bestS = 0;
+    bestMs = defaultMs;
+  }
+  h->tuneMinBlocks[key] = bestB;
+  h->tuneSplitLog2[key] = bestS;
+  h->tuneMs[key] = bestMs;
+  return NBK_OK;
+}
+
+NBK_API int nbk_get_tuning(nbk_handle h, unsigned flags, int* minBlocksPerSM, int* listSplit,
+                           float* ms) {
+  int rc = checkHandle(h, "nbk_get_tuning");
+  if (rc) return rc;
+  const int key = tuneKey(h, flags & ~(unsigned)(NBK_PAIRLIST | NBK_CORRECTIONS));
+  if (minBlocksPerSM) *minBlocksPerSM = h->tuneMinBlocks[key];
+  if (listSplit) *listSplit = 1 << h->tuneSplitLog2[key];
+  if (ms) *ms = h->tuneMs[key];
+  return NBK_OK;
+}
+
+NBK_API int nbk_set_tuning(nbk_handle h, unsigned flags, int minBlocksPerSM, int listSplit) {
+  int rc = checkHandle(h, "nbk_set_tuning");
+  if (rc) return rc;
+  if (minBlocksPerSM < 4 || minBlocksPerSM > 6)
+    return setErr(NBK_ERR_ARG, "nbk_set_tuning: minBlocksPerSM must be 4, 5 or 6");
+  int sl = -1;
+  for (int k = 0; k <= 2; ++k)
+    if (listSplit == (1 << k)) sl = k;
+  if (sl < 0) return setErr(NBK_ERR_ARG, "nbk_set_tuning: listSplit must be 1, 2 or 4");
+  const int key = tuneKey(h, flags & ~(unsigned)(NBK_PAIRLIST | NBK_CORRECTIONS));
+  h->tuneMinBlocks[key] = minBlocksPerSM;
+  h->tuneSplitLog2[key] = sl;
+  h->tuneMs[key] = 0.f;
   return NBK_OK;
 }

@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     finalizeKernel(int n, const long long* __restrict__ F, int stride,
                    const float4* __restrict__ xyzq, float4* __restrict__ outF,
                    float4* __restrict__ outS, int doSlow, int doVirial,
-                   long long* __restrict__ accBase, const int* __restrict__ slotRep) {
+                   long long* __restrict__ accBase, const int* __restrict__ slotRep,
+                   const ShiftVirialArgs shift) {
   long long v[18] = {};
   const int lane = threadIdx.x & 31;
   const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
@@ -319,6 +320,38 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     }
   }
   if (!doVirial) return;
+  // The lattice-shift part, (sum_i F_i) (x) shift for each compute, from the
+  // exact integer i-force sums of the compute (the split of
+  // reduceNonbondedVirialKernel / reduceVirialEnergyKernel,
+  // src/CudaComputeNonbondedKernel.cu:1649-1920). Each compute's product is
+  // rounded once, so the result does not depend on how lists were scheduled.
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < shift.numComputes;
+       c += gridDim.x * blockDim.x) {
+    const int rep = shift.compRep ? shift.compRep[c] : 0;
+    if (rep != curRep) {
+#pragma unroll
+      for (int p = 0; p < 18; ++p) {
+        if (v[p] != 0) atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
+        v[p] = 0;
+      }
+      curRep = rep;
+    }
+    const long long* F = shift.compF + 6 * (size_t)c;
+    const nbk_compute_record cr = shift.computes[c];
+    float3 la = shift.lata, lb = shift.latb, lc = shift.latc;
+    if (shift.compRep) {
+      la = shift.repLat[3 * rep];
+      lb = shift.repLat[3 * rep + 1];
+      lc = shift.repLat[3 * rep + 2];
+    }
+    const float3 sh = shiftOf(make_float3(cr.offsetXYZ.x, cr.offsetXYZ.y, cr.offsetXYZ.z), la, lb, lc);
+    const double S[3] = {(double)sh.x, (double)sh.y, (double)sh.z};
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      v[p] += toFixedEnergy((double)F[p / 3] * kForceScaleInv * S[p % 3]);
+      if (doSlow) v[9 + p] += toFixedEnergy((double)F[3 + p / 3] * kForceScaleInv * S[p % 3]);
+    }
+  }
   // Reduce the warp, then the block, before touching the 18 accumulator
   // words: every block adds each word once (per-warp adds only where a block
   // spans two replicas), which keeps same-address atomics off the critical path.
@@ -359,7 +392,8 @@ __global__ void __launch_bounds__(kFinalizeThreads)
 
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
-                                 int numSM, cudaStream_t st, const int* slotRep) {
+                                 int numSM, cudaStream_t st, const int* slotRep,
+                                 const ShiftVirialArgs* shift) {
   if (n <= 0) return cudaSuccess;
   const bool V = flags & NBK_VIRIAL;
   if (!V && !outF && !outS) return cudaSuccess;
@@ -368,9 +402,11 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
   // the FP64 energy/virial mode accumulates complete pair virials instead
   const bool atomVirial = V && !((flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64));
   if (!atomVirial && !outF && !outS) return cudaSuccess;
+  ShiftVirialArgs sv{};
+  if (shift && atomVirial) sv = *shift;
   finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS,
                                              (flags & NBK_SLOW) ? 1 : 0, atomVirial ? 1 : 0, acc,
-                                             slotRep);
+                                             slotRep, sv);
   return cudaGetLastError();
 }
 

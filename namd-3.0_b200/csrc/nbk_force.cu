@@ -20,15 +20,12 @@
 namespace nbk {
 
 constexpr int kForceWarps = 4;
+// FP32 mode: i-force and energy partials are folded into fixed point once per
+// group of kFoldTiles j tiles (groups counted from the start of the list; a
+// list's parts hold whole groups), so every sum is independent of the split.
+constexpr int kFoldTiles = 4;
 constexpr int kForceThreads = kForceWarps * kWarp;
 
-// The packed FP32 loop holds two pairs' state (and the FP64 energy mode its
-// FP64 pair virials): up to 96 registers
-// (20 warps per SM), the two independent pairs giving each warp its own ILP.
-#ifndef NBK_STEADY_MIN_BLOCKS
-#define NBK_STEADY_MIN_BLOCKS 5
-#endif
-constexpr int kSteadyMinBlocks = NBK_STEADY_MIN_BLOCKS;
 
 // Adds a warp's fixed-point accumulators to one replica's accumulator block.
 template <bool doEnergy, bool doVirial>
@@ -52,8 +49,13 @@ __device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& a
   npair = 0;
 }
 
-template <bool doEnergy, bool doVirial, bool doSlow, bool doE64, bool doBatch>
-__global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
+// MINB: CTAs per SM the register budget is cut for (4, 5 or 6 -> 128, 96 or
+// 80 registers; the packed loop holds two pairs' state, and 5 is the untuned
+// default); a.splitLog2: each list's j tiles are shared by 2^splitLog2
+// work items (warps), contiguous parts of equal tile count. Both are launch
+// choices of the autotuner; results do not depend on them (fixed-point sums).
+template <bool doEnergy, bool doVirial, bool doSlow, bool doE64, bool doBatch, int MINB>
+__global__ void __launch_bounds__(kForceThreads, MINB)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
@@ -61,6 +63,10 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
   // address per j serves all of its loads
   __shared__ float s_jt[kForceWarps][5][kWarp];
   __shared__ int s_type[kForceWarps][kWarp];
+  // FP32 mode: each lane's i force of the current list part in fixed point,
+  // folded in at the end of every j tile, so that the sums do not depend on
+  // how a list's tiles are split among warps
+  __shared__ long long s_fi[kForceWarps][6][kWarp];
 
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -76,18 +82,29 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
   // per-warp fixed-point accumulators: lane k < 9 owns virial[k], 9 <= k < 18
   // owns virialSlow[k-9]; lane 0 also owns the three energies.
   long long accE0 = 0, accE1 = 0, accE2 = 0, accVir = 0;
-  int npair = 0;  // interacting pairs seen by this lane (energy evaluations)
+  int npair = 0;
+  if (!doE64) {
+#pragma unroll
+    for (int q = 0; q < 6; ++q) s_fi[wib][q][lane] = 0;
+  }  // interacting pairs seen by this lane (energy evaluations)
   int curRep = 0;  // replica whose accumulators the warp is holding
 
   // lists are handed out one at a time from a global counter, so warps that
   // draw short lists keep working instead of idling at the end
+  const int split = 1 << a.splitLog2;
   for (;;) {
-    int L = 0;
-    if (lane == 0) L = atomicAdd(a.workCounter, 1);
-    L = __shfl_sync(0xffffffffu, L, 0);
-    if (L >= numLists) break;
+    int W = 0;
+    if (lane == 0) W = atomicAdd(a.workCounter, 1);
+    W = __shfl_sync(0xffffffffu, W, 0);
+    if (W >= numLists * split) break;
+    const int L = W >> a.splitLog2, part = W & (split - 1);
     const nbk_tile_list tl = a.lists[L];
     if (tl.jtileEnd < tl.jtileStart) continue;  // empty (warp-uniform)
+    const int chunk = ((((tl.jtileEnd - tl.jtileStart + split) >> a.splitLog2) + kFoldTiles - 1) /
+                       kFoldTiles) * kFoldTiles;
+    const int jtFirst = tl.jtileStart + part * chunk;
+    const int jtLast = min(tl.jtileEnd, jtFirst + chunk - 1);
+    if (jtLast < jtFirst) continue;  // this part has no tiles
     float3 la = a.lata, lb = a.latb, lc = a.latc;
     const float2* ljRow = nullptr;  // batched: this replica's LJ table (global)
     if (doBatch) {
@@ -122,13 +139,15 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
     const int ti = a.vdwTypes[iatom] * dim;
 
     float fix = 0.f, fiy = 0.f, fiz = 0.f, fisx = 0.f, fisy = 0.f, fisz = 0.f;
-    // steady state: two partial i sums per component (packed loop below)
+    // packed loop: this tile's two partial i sums per component
     float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
     float2 fisx2 = f2(0.f), fisy2 = f2(0.f), fisz2 = f2(0.f);
-    double eV = 0.0, eE = 0.0, eS = 0.0;
+    double eV = 0.0, eE = 0.0, eS = 0.0;         // FP64 energy mode, per list
+    long long eVq = 0, eEq = 0, eSq = 0;         // FP32 mode, fixed point per tile group
+    float eVg = 0.f, eEg = 0.f, eSg = 0.f;       // FP32 mode, the current tile group
     double wv[6] = {0, 0, 0, 0, 0, 0}, ws[6] = {0, 0, 0, 0, 0, 0};  // FP64 pair virials
 
-    for (int jt = tl.jtileStart; jt <= tl.jtileEnd; ++jt) {
+    for (int jt = jtFirst; jt <= jtLast; ++jt) {
       const int jstart = a.tileJatomStart[jt];
       const unsigned mask = a.tileExcls[jt].excl[lane];
       unsigned stepMask = __reduce_or_sync(0xffffffffu, mask);
@@ -326,40 +345,68 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
         atomicAddFixed(&a.force[5 * (size_t)a.stride + jatom], toFixedForce(fjsz));
       }
       if (doEnergy) {
-        eV += (double)eVt;
-        if (!doE64) {
-          eE += (double)eEt;
-          if (doSlow) eS += (double)eSt;
+        if (doE64) {
+          eV += (double)eVt;
+        } else {
+          eVg += eVt;
+          eEg += eEt;
+          if (doSlow) eSg += eSt;
+        }
+      }
+      if (!doE64 && ((((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0) || jt == jtLast)) {
+        // end of a tile group: its energies and i forces into fixed point
+        if (doEnergy) {
+          eVq += toFixedEnergyF(eVg);
+          eEq += toFixedEnergyF(eEg);
+          if (doSlow) eSq += toFixedEnergyF(eSg);
+          eVg = eEg = eSg = 0.f;
+        }
+        s_fi[wib][0][lane] += (long long)toFixedForce(fix2.x + fix2.y);
+        s_fi[wib][1][lane] += (long long)toFixedForce(fiy2.x + fiy2.y);
+        s_fi[wib][2][lane] += (long long)toFixedForce(fiz2.x + fiz2.y);
+        fix2 = fiy2 = fiz2 = f2(0.f);
+        if (doSlow) {
+          s_fi[wib][3][lane] += (long long)toFixedForce(fisx2.x + fisx2.y);
+          s_fi[wib][4][lane] += (long long)toFixedForce(fisy2.x + fisy2.y);
+          s_fi[wib][5][lane] += (long long)toFixedForce(fisz2.x + fisz2.y);
+          fisx2 = fisy2 = fisz2 = f2(0.f);
         }
       }
       __syncwarp();
     }  // jt
-    if (!doE64) {
-      fix = fix2.x + fix2.y;
-      fiy = fiy2.x + fiy2.y;
-      fiz = fiz2.x + fiz2.y;
-      fisx = fisx2.x + fisx2.y;
-      fisy = fisy2.x + fisy2.y;
-      fisz = fisz2.x + fisz2.y;
-    }
 
-    // i forces (fixed point) and the list's shift part of the virial
-    const unsigned long long qx = toFixedForce(fix), qy = toFixedForce(fiy), qz = toFixedForce(fiz);
-    if (fix != 0.f || fiy != 0.f || fiz != 0.f) {
+    // i forces (fixed point)
+    unsigned long long qx, qy, qz, sx = 0, sy = 0, sz = 0;
+    if (!doE64) {
+      qx = (unsigned long long)s_fi[wib][0][lane];
+      qy = (unsigned long long)s_fi[wib][1][lane];
+      qz = (unsigned long long)s_fi[wib][2][lane];
+      s_fi[wib][0][lane] = s_fi[wib][1][lane] = s_fi[wib][2][lane] = 0;
+      if (doSlow) {
+        sx = (unsigned long long)s_fi[wib][3][lane];
+        sy = (unsigned long long)s_fi[wib][4][lane];
+        sz = (unsigned long long)s_fi[wib][5][lane];
+        s_fi[wib][3][lane] = s_fi[wib][4][lane] = s_fi[wib][5][lane] = 0;
+      }
+    } else {
+      qx = toFixedForce(fix);
+      qy = toFixedForce(fiy);
+      qz = toFixedForce(fiz);
+      if (doSlow) {
+        sx = toFixedForce(fisx);
+        sy = toFixedForce(fisy);
+        sz = toFixedForce(fisz);
+      }
+    }
+    if (qx | qy | qz) {
       atomicAddFixed(&a.force[0 * (size_t)a.stride + iatom], qx);
       atomicAddFixed(&a.force[1 * (size_t)a.stride + iatom], qy);
       atomicAddFixed(&a.force[2 * (size_t)a.stride + iatom], qz);
     }
-    unsigned long long sx = 0, sy = 0, sz = 0;
-    if (doSlow) {
-      sx = toFixedForce(fisx);
-      sy = toFixedForce(fisy);
-      sz = toFixedForce(fisz);
-      if (fisx != 0.f || fisy != 0.f || fisz != 0.f) {
-        atomicAddFixed(&a.force[3 * (size_t)a.stride + iatom], sx);
-        atomicAddFixed(&a.force[4 * (size_t)a.stride + iatom], sy);
-        atomicAddFixed(&a.force[5 * (size_t)a.stride + iatom], sz);
-      }
+    if (doSlow && (sx | sy | sz)) {
+      atomicAddFixed(&a.force[3 * (size_t)a.stride + iatom], sx);
+      atomicAddFixed(&a.force[4 * (size_t)a.stride + iatom], sy);
+      atomicAddFixed(&a.force[5 * (size_t)a.stride + iatom], sz);
     }
     if (doVirial && doE64) {
       // FP64 mode: the complete pair virial of this list, W = -sum g d (x) d
@@ -379,7 +426,8 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
         if (lane < 9 || doSlow) accVir += toFixedEnergy(v);
       }
     } else if (doVirial && !zeroShift) {
-      // W[a][b] += (sum_i F_i)[a] * shift[b] for this list
+      // the lattice-shift part of the virial, (sum_i F_i) (x) shift, is formed
+      // per compute by shiftVirialKernel from these exact integer sums
       const long long Fx = warpSumLL((long long)qx), Fy = warpSumLL((long long)qy),
                       Fz = warpSumLL((long long)qz);
       long long Gx = 0, Gy = 0, Gz = 0;
@@ -388,23 +436,33 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
         Gy = warpSumLL((long long)sy);
         Gz = warpSumLL((long long)sz);
       }
-      if (lane < 18) {
-        const int comp = lane % 9;
-        const int ca = comp / 3, cb = comp % 3;
-        long long Fa;
-        if (lane < 9) Fa = (ca == 0) ? Fx : (ca == 1) ? Fy : Fz;
-        else Fa = (ca == 0) ? Gx : (ca == 1) ? Gy : Gz;
-        const float s_b = (cb == 0) ? sh.x : (cb == 1) ? sh.y : sh.z;
-        if (lane < 9 || doSlow)
-          accVir += toFixedEnergy((double)Fa * kForceScaleInv * (double)s_b);
+      long long* cf = a.compF + 6 * (size_t)tl.icompute;
+      if (lane == 0) {
+        if (Fx) atomicAddFixed(&cf[0], (unsigned long long)Fx);
+        if (Fy) atomicAddFixed(&cf[1], (unsigned long long)Fy);
+        if (Fz) atomicAddFixed(&cf[2], (unsigned long long)Fz);
+        if (doSlow) {
+          if (Gx) atomicAddFixed(&cf[3], (unsigned long long)Gx);
+          if (Gy) atomicAddFixed(&cf[4], (unsigned long long)Gy);
+          if (Gz) atomicAddFixed(&cf[5], (unsigned long long)Gz);
+        }
       }
     }
     if (doEnergy) {
-      const double sV = warpSumD(eV), sE = warpSumD(eE), sS = doSlow ? warpSumD(eS) : 0.0;
+      long long sV, sE, sS = 0;
+      if (doE64) {
+        sV = toFixedEnergy(warpSumD(eV));
+        sE = toFixedEnergy(warpSumD(eE));
+        if (doSlow) sS = toFixedEnergy(warpSumD(eS));
+      } else {
+        sV = warpSumLL(eVq);
+        sE = warpSumLL(eEq);
+        if (doSlow) sS = warpSumLL(eSq);
+      }
       if (lane == 0) {
-        accE0 += toFixedEnergy(sV);
-        accE1 += toFixedEnergy(sE);
-        accE2 += toFixedEnergy(sS);
+        accE0 += sV;
+        accE1 += sE;
+        accE2 += sS;
       }
     }
   }  // lists
@@ -415,10 +473,10 @@ __global__ void __launch_bounds__(kForceThreads, kSteadyMinBlocks)
                                 accVir, npair);
 }
 
-template <bool E, bool V, bool S, bool D, bool B>
+template <bool E, bool V, bool S, bool D, bool B, int MINB>
 static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
   const size_t shmem = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
-  auto k = forceKernel<E, V, S, D, B>;
+  auto k = forceKernel<E, V, S, D, B, MINB>;
   static int cachedDim = -1, cachedBlocks = 0;
   if (cachedDim != a.c.ljDim) {
     if (shmem > 48 * 1024) {
@@ -435,7 +493,18 @@ static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st) {
+template <bool E, bool V, bool S, bool D, bool B>
+static cudaError_t launchShape(const ForceArgs& a, int minBlocks, int numSM, cudaStream_t st) {
+  switch (minBlocks) {
+    case 4: return launchT<E, V, S, D, B, 4>(a, numSM, st);
+    case 5: return launchT<E, V, S, D, B, 5>(a, numSM, st);
+    case 6: return launchT<E, V, S, D, B, 6>(a, numSM, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int numSM,
+                        cudaStream_t st) {
   const bool E = flags & NBK_ENERGY;
   const bool B = a.compRep != nullptr;
   const int idx = (B ? 16 : 0) | (E ? 8 : 0) | ((flags & NBK_VIRIAL) ? 4 : 0) |
@@ -443,7 +512,7 @@ cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStrea
   switch (idx) {
 #define NBK_CASE(i, e, v, s, d, b) \
   case i:                          \
-    return launchT<e, v, s, d, b>(a, numSM, st);
+    return launchShape<e, v, s, d, b>(a, minBlocks, numSM, st);
     NBK_CASE(0, false, false, false, false, false)
     NBK_CASE(2, false, false, true, false, false)
     NBK_CASE(4, false, true, false, false, false)

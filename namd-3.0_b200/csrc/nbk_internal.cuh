@@ -303,6 +303,12 @@ __device__ __forceinline__ long long toFixedEnergy(double v) {
   return __double2ll_rn(v * kEnergyScale);
 }
 
+// The same conversion from FP32: v * 2^30 is exact, so the result equals
+// toFixedEnergy((double)v).
+__device__ __forceinline__ long long toFixedEnergyF(float v) {
+  return __float2ll_rn(v * 1073741824.0f);
+}
+
 __device__ __forceinline__ void atomicAddFixed(long long* p, unsigned long long v) {
   atomicAdd(reinterpret_cast<unsigned long long*>(p), v);
 }
@@ -341,7 +347,9 @@ struct ForceArgs {
   long long* force;            // SoA [6][stride] fixed point
   int stride;
   long long* acc;              // [kAccCount]
-  int* workCounter;            // next list to hand out (zeroed before the launch)
+  int* workCounter;            // next work item to hand out (zeroed before the launch)
+  int splitLog2;               // force kernel: 2^splitLog2 work items per list
+  long long* compF;            // FP32 mode with virial: [numComputes][6] i-force sums per compute
   NbkConst64 c64;              // FP64 energy/virial mode
   // replicas (batched evaluation; all NULL for a single system)
   const int* compRep;          // [numComputes] replica of each compute

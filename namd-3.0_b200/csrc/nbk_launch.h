@@ -7,7 +7,9 @@
 
 namespace nbk {
 
-cudaError_t launchForce(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st);
+// minBlocks: 4, 5 or 6 CTAs per SM (the register cap); a.splitLog2 set by the caller.
+cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int numSM,
+                        cudaStream_t st);
 // Pairlist refinement of the culled lists a.lists[0, a.numListsHost): writes
 // a.tileExcls, a.jtileActive, a.listActive and the excluded-pair counts.
 cudaError_t launchRefine(const ForceArgs& a, int numSM, cudaStream_t st);
@@ -46,9 +48,22 @@ struct CorrArgs {
 };
 cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st);
 
+// The lattice-shift part of the virial, (sum_i F_i) (x) shift per compute,
+// from the exact integer i-force sums the force kernel leaves per compute.
+struct ShiftVirialArgs {
+  int numComputes;
+  const long long* compF;                // [numComputes][6]
+  const nbk_compute_record* computes;
+  float3 lata, latb, latc;
+  const int* compRep;                    // batched replicas, else NULL
+  const float3* repLat;
+};
+
+// shift: also folds the shift virial into the accumulators (FP32 virial mode).
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
-                                 int numSM, cudaStream_t st, const int* slotRep = nullptr);
+                                 int numSM, cudaStream_t st, const int* slotRep = nullptr,
+                                 const ShiftVirialArgs* shift = nullptr);
 
 // Converts numReplicas accumulator blocks into numReplicas nbk_virial_energy records.
 cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st,

@@ -348,6 +348,9 @@ def dev_lib() -> C.CDLL:
         lib.nbk_get_tile_list_stat.argtypes = [vp, C.POINTER(TileListStat), vp]
         lib.nbk_export_tile_lists.argtypes = [vp, C.POINTER(i), C.POINTER(i), vp, vp, vp, vp]
         lib.nbk_set_kernel_timing.argtypes = [vp, i]
+        lib.nbk_autotune.argtypes = [vp, u, i, vp]
+        lib.nbk_get_tuning.argtypes = [vp, u, C.POINTER(i), C.POINTER(i), C.POINTER(C.c_float)]
+        lib.nbk_set_tuning.argtypes = [vp, u, i, i]
         lib.nbk_get_kernel_times.argtypes = [vp, C.POINTER(C.c_float), i, C.POINTER(i)]
         lib.nbk_launch_count.restype = C.c_longlong
         lib.nbk_launch_count.argtypes = [vp]
@@ -542,6 +545,24 @@ class Nonbonded:
         n = C.c_longlong(0)
         _dcheck(dev_lib().nbk_get_pair_count(self._h, C.byref(n), stream), "nbk_get_pair_count")
         return int(n.value)
+
+    def autotune(self, flags=NBK_ENERGY | NBK_VIRIAL | NBK_SLOW, iterations=5, stream=None):
+        """Times the force kernel's launch shapes on the current refined lists and
+        keeps the fastest for these flags (nbk_autotune); returns the choice."""
+        _dcheck(dev_lib().nbk_autotune(self._h, flags, iterations, stream), "nbk_autotune")
+        return self.tuning(flags)
+
+    def set_tuning(self, flags, ctas_per_sm, warps_per_list):
+        """Pins the force kernel's launch shape for these flags (nbk_set_tuning)."""
+        _dcheck(dev_lib().nbk_set_tuning(self._h, flags, ctas_per_sm, warps_per_list),
+                "nbk_set_tuning")
+
+    def tuning(self, flags=NBK_ENERGY | NBK_VIRIAL | NBK_SLOW):
+        """(CTAs per SM, warps per tile list, ms per force launch) for these flags."""
+        b, sp, ms = C.c_int(0), C.c_int(0), C.c_float(0)
+        _dcheck(dev_lib().nbk_get_tuning(self._h, flags, C.byref(b), C.byref(sp), C.byref(ms)),
+                "nbk_get_tuning")
+        return {"ctas_per_sm": b.value, "warps_per_list": sp.value, "ms": ms.value}
 
     def export_tile_lists(self, stream=None):
         nl, nj = C.c_int(0), C.c_int(0)
