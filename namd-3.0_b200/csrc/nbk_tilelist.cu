@@ -171,12 +171,32 @@ __global__ void compactKernel(int numLists, const nbk_tile_list* __restrict__ sr
 // in place, jtileActive / listActive for the compaction and the per-replica
 // count of excluded pairs within the pairlist cutoff. One warp per list,
 // lists handed out from a.workCounter.
+//
+// Layout of the work: every lane tests its i atom against j = 0..31 in
+// natural order, two j atoms (k, k + 16) per packed-FP32 step, with the j
+// tile's coordinates and indices read as warp-wide broadcasts from shared
+// memory. The sign bits of r^2 - plcutoff^2 (the same per-element rounding
+// as dist2; the sign of a rounded difference is the sign of the exact one)
+// are shifted into a word whose bit j marks pair (lane, j); one rotation by
+// the lane number turns it into the TileExcl order (bit t <-> j = (lane + t)
+// & 31). Exclusions are only looked up for candidates whose global indices
+// lie within the i atom's maxdiff window: |jIndex - iIndex| <= maxdiff is
+// tested as the sign of (jIndex - iIndex)^2 - (maxdiff^2 + 1/2) in FP32,
+// exact while indices are below 2^24 and maxdiff <= kFpWindowMaxDiff (the
+// difference and maxdiff^2 + 1/2 are then representable, and a fused
+// multiply-add rounds once and keeps the sign). Outside those bounds every
+// candidate is looked up.
+constexpr int kFpWindowMaxDiff = 2896;  // 2896^2 + 1/2 < 2^23
+
 __global__ void __launch_bounds__(128) refineKernel(const __grid_constant__ ForceArgs a) {
-  __shared__ float4 s_xyzq[4][32];
+  // per warp: s_p0[k] = (x_k, x_k+16, y_k, y_k+16), s_p1[k] = (z_k, z_k+16, index_k, index_k+16)
+  __shared__ float4 s_p0[4][16], s_p1[4][16];
   __shared__ int s_jidx[4][32];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
-  const float plc2 = a.c.plcutoff2;
+  const float2 nPlc2 = f2(-a.c.plcutoff2);
+  float* const p0 = reinterpret_cast<float*>(&s_p0[wib][lane & 15]) + (lane >> 4);
+  float* const p1 = reinterpret_cast<float*>(&s_p1[wib][lane & 15]) + (lane >> 4);
   int nexcl = 0, curRep = 0;
   for (;;) {
     int L = 0;
@@ -212,42 +232,80 @@ __global__ void __launch_bounds__(128) refineKernel(const __grid_constant__ Forc
     if (lane >= nloopi) xi.x = xi.y = xi.z = -1.0e10f;
     const int iIndex = a.atomIndex[iatom];
     const int2 em = a.exclIndexMaxDiff[iatom];
+    const bool fpList = __all_sync(0xffffffffu, lane >= nloopi || ((unsigned)iIndex < (1u << 24) &&
+                                                                    em.y <= kFpWindowMaxDiff));
+    const float emy = (float)min(max(em.y, 0), kFpWindowMaxDiff);
+    const float2 nXi = f2(-xi.x), nYi = f2(-xi.y), nZi = f2(-xi.z);
+    const float2 nIi = f2(-(float)iIndex), nT = f2(-fmaf(emy, emy, 0.5f));
     int activeTiles = 0;
-    for (int jt = tl.jtileStart; jt <= tl.jtileEnd; ++jt) {
-      const int jstart = a.tileJatomStart[jt];
-      const bool diag = selfCompute && (jstart == tl.iatomStart);
-      const int nloopj = min(pp.jatomSize - jstart, 32);
-      const int nfreej = max(pp.jatomFreeSize - jstart, 0);
-      float4 xj = a.xyzq[jstart + lane];
-      if (lane >= nloopj) xj.x = xj.y = xj.z = 1.0e10f;
-      s_xyzq[wib][lane] = xj;
-      s_jidx[wib][lane] = a.atomIndex[jstart + lane];
-      __syncwarp();
-      unsigned m = 0;
-#pragma unroll 4
-      for (int t = 0; t < 32; ++t) {
-        const int j = (lane + t) & 31;
-        const float4 x = s_xyzq[wib][j];
-        const float r2 = dist2(__fsub_rn(x.x, xi.x), __fsub_rn(x.y, xi.y), __fsub_rn(x.z, xi.z));
-        const bool cand = (diag ? (t > 0 && lane + t < 32) : true) && (r2 < plc2) &&
-                          (j < nfreej || lane < nfreei);
-        if (cand) {
-          bool excluded = false;
+    for (int jt0 = tl.jtileStart; jt0 <= tl.jtileEnd; jt0 += 32) {
+      const int nt = min(32, tl.jtileEnd - jt0 + 1);
+      const int jsLane = lane < nt ? a.tileJatomStart[jt0 + lane] : 0;
+      // software pipeline: the next tile's atoms are loaded before this tile's math
+      int jsNext = __shfl_sync(0xffffffffu, jsLane, 0);
+      float4 xjNext = a.xyzq[jsNext + lane];
+      int idxNext = a.atomIndex[jsNext + lane];
+      for (int u = 0; u < nt; ++u) {
+        const int jt = jt0 + u;
+        const int jstart = jsNext;
+        float4 xj = xjNext;
+        const int jIndex = idxNext;
+        if (u + 1 < nt) {  // warp-uniform
+          jsNext = __shfl_sync(0xffffffffu, jsLane, u + 1);
+          xjNext = a.xyzq[jsNext + lane];
+          idxNext = a.atomIndex[jsNext + lane];
+        }
+        const bool diag = selfCompute && (jstart == tl.iatomStart);
+        const int nloopj = min(pp.jatomSize - jstart, 32);
+        const int nfreej = max(pp.jatomFreeSize - jstart, 0);
+        if (lane >= nloopj) xj.x = xj.y = xj.z = 1.0e10f;
+        p0[0] = xj.x;
+        p0[2] = xj.y;
+        p1[0] = xj.z;
+        p1[2] = (float)jIndex;
+        s_jidx[wib][lane] = jIndex;
+        const bool fpTile = fpList && __all_sync(0xffffffffu, lane >= nloopj || (unsigned)jIndex < (1u << 24));
+        __syncwarp();
+        unsigned cA = 0, cB = 0, wA = 0, wB = 0;
+#pragma unroll
+        for (int k = 15; k >= 0; --k) {
+          const float4 P0 = s_p0[wib][k], P1 = s_p1[wib][k];
+          const float2 DX = add2(make_float2(P0.x, P0.y), nXi);
+          const float2 DY = add2(make_float2(P0.z, P0.w), nYi);
+          const float2 DZ = add2(make_float2(P1.x, P1.y), nZi);
+          const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+          const float2 C = add2(R2, nPlc2);  // negative: within the pairlist cutoff
+          const float2 DI = add2(make_float2(P1.z, P1.w), nIi);
+          const float2 W = fma2(DI, DI, nT);  // negative: within the maxdiff window
+          cA = __funnelshift_l(__float_as_uint(C.x), cA, 1);
+          cB = __funnelshift_l(__float_as_uint(C.y), cB, 1);
+          wA = __funnelshift_l(__float_as_uint(W.x), wA, 1);
+          wB = __funnelshift_l(__float_as_uint(W.y), wB, 1);
+        }
+        unsigned mw = cA | (cB << 16);  // bit j: pair (lane, j) within the pairlist cutoff
+        if (diag) mw &= 0xFFFFFFFEu << lane;                          // self tile: j > lane only
+        if (lane >= nfreei && nfreej < 32) mw &= (1u << nfreej) - 1u;  // fixed-fixed pairs
+        unsigned need = fpTile ? (mw & (wA | (wB << 16))) : mw;
+        while (need) {
+          const int j = __ffs(need) - 1;
+          need &= need - 1u;
           const int diff = s_jidx[wib][j] - iIndex;
           if (abs(diff) <= em.y) {
             const unsigned bit = (unsigned)(diff + em.x);
             const unsigned w = ((int)(bit >> 5) < a.numExclWords) ? __ldg(&a.exclBits[bit >> 5]) : 0u;
-            excluded = (w >> (bit & 31)) & 1u;
+            if ((w >> (bit & 31)) & 1u) {
+              mw &= ~(1u << j);
+              ++nexcl;
+            }
           }
-          if (excluded) ++nexcl;
-          else m |= 1u << t;
         }
+        const unsigned m = __funnelshift_r(mw, mw, lane);  // bit t <-> j = (lane + t) & 31
+        a.tileExcls[jt].excl[lane] = m;
+        const bool any = __any_sync(0xffffffffu, m != 0);
+        if (lane == 0) a.jtileActive[jt] = any ? 1 : 0;
+        activeTiles += any ? 1 : 0;
+        __syncwarp();
       }
-      a.tileExcls[jt].excl[lane] = m;
-      const bool any = __any_sync(0xffffffffu, m != 0);
-      if (lane == 0) a.jtileActive[jt] = any ? 1 : 0;
-      activeTiles += any ? 1 : 0;
-      __syncwarp();
     }
     if (lane == 0) a.listActive[L] = activeTiles;
   }

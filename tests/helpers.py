@@ -87,3 +87,79 @@ def real_slots(packed):
     mask = np.zeros(packed.atomStorageSize, dtype=bool)
     mask[packed.slotOfAtom] = True
     return mask
+
+
+# ---------------------------------------------------------------------------
+# packed-system variants for the pairlist refinement's edge cases
+# ---------------------------------------------------------------------------
+class PackedVariant:
+    """A Packed system with some of its arrays replaced: the attributes the
+    oracle and the reference harness read and the view the device library
+    reads both point at the replacements. Only for test inputs."""
+
+    _FIELDS = {"atomIndex": "atomIndex", "exclIndexMaxDiff": "exclIndexMaxDiff",
+               "exclusionBits": "exclusionBits", "patches": "patches"}
+
+    def __init__(self, packed, **arrays):
+        self.__dict__.update(packed.__dict__)
+        self._base = packed            # keeps the host-side storage alive
+        self._keep = []
+        v = nbk.PackedView.from_buffer_copy(packed.v)
+        for name, arr in arrays.items():
+            arr = np.ascontiguousarray(arr, dtype=np.uint32 if name == "exclusionBits" else np.int32)
+            self._keep.append(arr)
+            setattr(self, name, arr)
+            field = self._FIELDS[name]
+            setattr(v, field, arr.ctypes.data_as(type(getattr(v, field))))
+            if name == "exclusionBits":
+                v.numExclusionWords = len(arr)
+        self.v = v
+
+
+def exclusion_lists(system):
+    """Per atom: the sorted offsets {0} U {partner - atom} of its full exclusions."""
+    partners = [[0] for _ in range(system.natoms)]
+    for x, y in system.arrays()["fullExcl"]:
+        partners[x].append(int(y) - int(x))
+        partners[y].append(int(x) - int(y))
+    return partners
+
+
+def renumbered(packed, perm):
+    """The packed system with global atom index g renamed perm[g]: atomIndex
+    and the (base, maxdiff) exclusion bit array re-encoded for the new
+    numbering, so that exactly the same pairs stay excluded."""
+    offs = exclusion_lists(packed.system)
+    lists, base, maxdiff, total = {}, [], [], 0
+    atom_list = np.empty(len(offs), dtype=np.int64)
+    for a, lst in enumerate(offs):
+        key = tuple(sorted({int(perm[a + d]) - int(perm[a]) for d in lst}))
+        k = lists.get(key)
+        if k is None:
+            k = lists[key] = len(base)
+            md = max(-key[0], key[-1])
+            base.append(total + md)
+            maxdiff.append(md)
+            total += 2 * md + 1
+        atom_list[a] = k
+    bits = np.zeros((total + 31) // 32, dtype=np.uint32)
+    for key, k in lists.items():
+        for d in key:
+            b = base[k] + d
+            bits[b >> 5] |= np.uint32(1 << (b & 31))
+    old = packed.atomIndex.astype(np.int64)
+    em = np.stack([np.asarray(base, np.int64)[atom_list[old]],
+                   np.asarray(maxdiff, np.int64)[atom_list[old]]], axis=1)
+    return PackedVariant(packed, atomIndex=np.asarray(perm, np.int64)[old], exclIndexMaxDiff=em,
+                         exclusionBits=bits)
+
+
+def molecule_boundaries(system):
+    """Global indices b such that no full exclusion joins an atom below b to
+    one at or above b."""
+    cross = np.zeros(system.natoms + 1, dtype=np.int64)
+    for x, y in system.arrays()["fullExcl"]:
+        lo, hi = min(x, y), max(x, y)
+        cross[lo + 1] += 1
+        cross[hi + 1] -= 1
+    return np.flatnonzero(np.cumsum(cross) == 0)
