@@ -59,9 +59,10 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
-  // packed loop: the j tile as five rows (x, y, z, q, type bits) so that one
-  // address per j serves all of its loads
-  __shared__ float s_jt[kForceWarps][5][kWarp];
+  // packed loop: the j tile as five rows (x, y, z, q, type bits), each stored
+  // twice in a row (entries j and j + 32) so that j = (lane + k) & 31 and
+  // j ^ 16 are the fixed offsets lane + k and lane + k + 16 from one address
+  __shared__ float s_jt[kForceWarps][5][2 * kWarp];
   __shared__ int s_type[kForceWarps][kWarp];
   // FP32 mode: each lane's i force of the current list part in fixed point,
   // folded in at the end of every j tile, so that the sums do not depend on
@@ -154,11 +155,12 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
       if (stepMask == 0) continue;
       const float4 xj = a.xyzq[jstart + lane];
       if constexpr (!doE64) {
-        s_jt[wib][0][lane] = xj.x;
-        s_jt[wib][1][lane] = xj.y;
-        s_jt[wib][2][lane] = xj.z;
-        s_jt[wib][3][lane] = xj.w;
-        s_jt[wib][4][lane] = __int_as_float(a.vdwTypes[jstart + lane]);
+        const float tyj = __int_as_float(a.vdwTypes[jstart + lane]);
+        s_jt[wib][0][lane] = s_jt[wib][0][lane + kWarp] = xj.x;
+        s_jt[wib][1][lane] = s_jt[wib][1][lane + kWarp] = xj.y;
+        s_jt[wib][2][lane] = s_jt[wib][2][lane + kWarp] = xj.z;
+        s_jt[wib][3][lane] = s_jt[wib][3][lane + kWarp] = xj.w;
+        s_jt[wib][4][lane] = s_jt[wib][4][lane + kWarp] = tyj;
       } else {
         s_xyzq[wib][lane] = xj;
       }
@@ -184,22 +186,22 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
 #pragma unroll 2
         for (int k = 0; k < 16; ++k, mk >>= 1) {
           if (!((stepMask >> k) & 0x10001u)) continue;  // warp-uniform
-          const int jA = (lane + k) & 31, jB = jA ^ 16;
-          const float* pA = &s_jt[wib][0][jA];
-          const float* pB = &s_jt[wib][0][jB];
+          // element x: j = (lane + k) & 31, element y: j ^ 16
+          const float* pA = &s_jt[wib][0][lane + k];
+          const float* pB = pA + 16;
           const float2 X = make_float2(pA[0], pB[0]);
-          const float2 Y = make_float2(pA[32], pB[32]);
-          const float2 Z = make_float2(pA[64], pB[64]);
+          const float2 Y = make_float2(pA[64], pB[64]);
+          const float2 Z = make_float2(pA[128], pB[128]);
           const float2 DX = add2(X, nXi), DY = add2(Y, nYi), DZ = add2(Z, nZi);
           const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
           const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
           const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
           if (!__any_sync(0xffffffffu, aA || aB)) continue;
           if (doEnergy) npair += (int)aA + (int)aB;
-          const int tyA = __float_as_int(pA[128]), tyB = __float_as_int(pB[128]);
+          const int tyA = __float_as_int(pA[256]), tyB = __float_as_int(pB[256]);
           const float2 abA = doBatch ? __ldg(&ljRow[ti + tyA]) : s_lj[ti + tyA];
           const float2 abB = doBatch ? __ldg(&ljRow[ti + tyB]) : s_lj[ti + tyB];
-          const float2 QQ = mul2(f2(xi.w), make_float2(pA[96], pB[96]));
+          const float2 QQ = mul2(f2(xi.w), make_float2(pA[192], pB[192]));
           const float2 r2s = make_float2(aA ? R2.x : c.cutoff2, aB ? R2.y : c.cutoff2);
           const float2 qqs = make_float2(aA ? QQ.x : 0.f, aB ? QQ.y : 0.f);
           const float2 As = make_float2(aA ? abA.x : 0.f, aB ? abB.x : 0.f);

@@ -118,45 +118,68 @@ __global__ void buildListsKernel(int numLists, const ListSeed* __restrict__ seed
 
 // After the pairlist refinement: drop j tiles without interacting pairs and
 // lists left empty (reSortTileLists' compaction, src/CudaTileListKernel.cu:
-// 1605-1665). counters[0] = lists kept, counters[1] = j tiles kept.
-__global__ void compactKernel(int numLists, const nbk_tile_list* __restrict__ src,
-                              const int* __restrict__ listActive, const int* __restrict__ jtileActive,
-                              const int* __restrict__ jatomSrc,
-                              const nbk_tile_excl* __restrict__ exclSrc,
-                              nbk_tile_list* __restrict__ dst, int* __restrict__ jatomDst,
-                              nbk_tile_excl* __restrict__ exclDst, int* __restrict__ counters) {
+// 1605-1665). counters[0] = lists kept, counters[1] = j tiles kept. A block
+// of kCompactWarps warps takes as many lists at a time, one per warp; one
+// thread reserves the output of all of them with one pair of atomics.
+constexpr int kCompactWarps = 8;
+
+__global__ void __launch_bounds__(kCompactWarps * 32)
+    compactKernel(int numLists, const nbk_tile_list* __restrict__ src,
+                  const int* __restrict__ listActive, const int* __restrict__ jtileActive,
+                  const int* __restrict__ jatomSrc, const nbk_tile_excl* __restrict__ exclSrc,
+                  nbk_tile_list* __restrict__ dst, int* __restrict__ jatomDst,
+                  nbk_tile_excl* __restrict__ exclDst, int* __restrict__ counters) {
+  __shared__ int s_n[kCompactWarps], s_pos[kCompactWarps], s_jpos[kCompactWarps];
   const int lane = threadIdx.x & 31;
-  const int warpsPerGrid = (gridDim.x * blockDim.x) >> 5;
-  for (int L = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; L < numLists; L += warpsPerGrid) {
-    const int n = listActive[L];
-    if (n == 0) continue;
-    const nbk_tile_list s = src[L];
-    if (s.jtileEnd < s.jtileStart) continue;
-    int pos = 0, jpos = 0;
-    if (lane == 0) {
-      pos = atomicAdd(&counters[0], 1);
-      jpos = atomicAdd(&counters[1], n);
+  const int wib = threadIdx.x >> 5;
+  for (int Lb = blockIdx.x * kCompactWarps; Lb < numLists; Lb += gridDim.x * kCompactWarps) {
+    const int L = Lb + wib;
+    int n = 0;
+    nbk_tile_list s;
+    if (L < numLists) {
+      s = src[L];
+      // listActive is only written for lists with tiles (empty lists skip the refinement)
+      if (s.jtileEnd >= s.jtileStart) n = listActive[L];
     }
-    pos = __shfl_sync(0xffffffffu, pos, 0);
-    jpos = __shfl_sync(0xffffffffu, jpos, 0);
-    int w = 0;
-    for (int j0 = s.jtileStart; j0 <= s.jtileEnd; j0 += 32) {
-      const int jt = j0 + lane;
-      const bool act = (jt <= s.jtileEnd) && jtileActive[jt];
-      unsigned ball = __ballot_sync(0xffffffffu, act);
-      if (act) jatomDst[jpos + w + __popc(ball & ((1u << lane) - 1u))] = jatomSrc[jt];
-      while (ball) {
-        const int b = __ffs(ball) - 1;
-        ball &= ball - 1;
-        exclDst[jpos + w].excl[lane] = exclSrc[j0 + b].excl[lane];
-        ++w;
+    if (lane == 0) s_n[wib] = n;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int kept = 0, tiles = 0;
+      for (int w = 0; w < kCompactWarps; ++w) {
+        s_pos[w] = kept;
+        s_jpos[w] = tiles;
+        kept += s_n[w] > 0 ? 1 : 0;
+        tiles += s_n[w];
+      }
+      const int p0 = kept ? atomicAdd(&counters[0], kept) : 0;
+      const int j0 = kept ? atomicAdd(&counters[1], tiles) : 0;
+      for (int w = 0; w < kCompactWarps; ++w) {
+        s_pos[w] += p0;
+        s_jpos[w] += j0;
       }
     }
-    if (lane == 0) {
-      nbk_tile_list d = s;
-      d.jtileStart = jpos;
-      d.jtileEnd = jpos + n - 1;
-      dst[pos] = d;
+    __syncthreads();
+    if (n > 0) {  // warp-uniform
+      const int pos = s_pos[wib], jpos = s_jpos[wib];
+      int w = 0;
+      for (int j0 = s.jtileStart; j0 <= s.jtileEnd; j0 += 32) {
+        const int jt = j0 + lane;
+        const bool act = (jt <= s.jtileEnd) && jtileActive[jt];
+        unsigned ball = __ballot_sync(0xffffffffu, act);
+        if (act) jatomDst[jpos + w + __popc(ball & ((1u << lane) - 1u))] = jatomSrc[jt];
+        while (ball) {
+          const int b = __ffs(ball) - 1;
+          ball &= ball - 1;
+          exclDst[jpos + w].excl[lane] = exclSrc[j0 + b].excl[lane];
+          ++w;
+        }
+      }
+      if (lane == 0) {
+        nbk_tile_list d = s;
+        d.jtileStart = jpos;
+        d.jtileEnd = jpos + n - 1;
+        dst[pos] = d;
+      }
     }
   }
 }
@@ -354,9 +377,8 @@ cudaError_t launchCompact(int numLists, const nbk_tile_list* src, const int* lis
                           nbk_tile_list* dst, int* jatomDst, nbk_tile_excl* exclDst, int* counters,
                           int numSM, cudaStream_t st) {
   if (numLists <= 0) return cudaSuccess;
-  const int threads = 256;
-  const int blocks = min((numLists + 7) / 8, numSM * 8);
-  compactKernel<<<blocks, threads, 0, st>>>(numLists, src, listActive, jtileActive, jatomSrc,
+  const int blocks = min((numLists + kCompactWarps - 1) / kCompactWarps, numSM * 8);
+  compactKernel<<<blocks, kCompactWarps * 32, 0, st>>>(numLists, src, listActive, jtileActive, jatomSrc,
                                             exclSrc, dst, jatomDst, exclDst, counters);
   return cudaGetLastError();
 }
