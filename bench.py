@@ -197,6 +197,44 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+def resident_timing(sys_, packed, local_rank, stream, reps=20):
+    """GPU-resident input marshaling on this workload: the device patch sort,
+    the patch-centred xyzq and the per-slot types / exclusion indices, each
+    timed with CUDA events (mean of `reps` launches), beside the host packing
+    of the same positions (nbk_pack_update_positions, one thread)."""
+    import torch
+    import nbk
+    dev = torch.device("cuda", local_rank)
+    st = stream.cuda_stream
+    lay = nbk.ResidentLayout(sys_, packed, device=local_rank)
+    order = torch.zeros(len(lay.ids), dtype=torch.int32, device=dev)
+    xyzq = torch.zeros((packed.atomStorageSize, 4), dtype=torch.float32, device=dev)
+    h = nbk.Nonbonded(nbk.NonbondedParams(), sys_.lj_table(), local_rank)
+    h.setup(packed, stream=st)
+    h.set_exclusions_by_atom(lay.excl_by_atom)
+    calls = {"sort_us": lambda: lay.sort_patch_atoms(order, stream=st),
+             "positions_us": lambda: lay.set_compute_positions(order, xyzq, stream=st),
+             "types_excl_us": lambda: h.update_vdw_types_excl_device(lay, order, stream=st)}
+    out = {}
+    for name, fn in calls.items():
+        fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        out[name] = a.elapsed_time(b) * 1e3 / reps
+    h.close()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        packed.update_positions()
+    out["host_packing_us"] = (time.perf_counter() - t0) / 3 * 1e6
+    out["patches"] = int(lay.numPatches)
+    out["max_patch_atoms"] = int(lay.records[:, 3].max())
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import nbk
@@ -337,6 +375,8 @@ def run_gpu(args, rank, world, local_rank):
     e2e = {"value": e2e_pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
            "d2h_bytes_per_step": 2 * 16 * n + 8 * 31, "steps": ke}
 
+    resident = resident_timing(sys_, packed, local_rank, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_eval_sample(packed, args.cpu_seconds)
@@ -355,6 +395,7 @@ def run_gpu(args, rank, world, local_rank):
             "evals_per_s": args.steps / (total_ms * 1e-3) * world,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks,
+            "resident_marshaling": resident,
             "wall_s_timed_region": wall,
         }
         print(json.dumps(out))

@@ -351,6 +351,90 @@ NBK_API int nbk_get_tuning(nbk_handle h, unsigned flags, int* minBlocksPerSM, in
  * 5 or 6; 1, 2 or 4 warps per tile list). */
 NBK_API int nbk_set_tuning(nbk_handle h, unsigned flags, int minBlocksPerSM, int listSplit);
 
+/* ---- GPU-resident input marshaling -------------------------------------------
+ * For callers whose atoms stay on the device between steps (NAMD's
+ * GPU-resident integrator, SequencerCUDA with device migration): the patch
+ * atom order, the patch-centred xyzq and the per-slot vdW types / exclusion
+ * indices are produced by kernels from the integrator's per-atom arrays
+ * instead of host loops and copies. The per-atom arrays are in "buffer
+ * order": patch p's atoms occupy [bufferOffset, bufferOffset + numAtoms) of
+ * every per-atom array, in any order; its nonbonded slots are
+ * [bufferOffsetNBPad, bufferOffsetNBPad + numAtomsNBPad). All pointers named
+ * d_* are device pointers. */
+
+/* CudaLocalRecord, src/CudaRecord.h:35-52 (128 bytes; the five CudaPeerRecords
+ * are carried as opaque words). Only patchID..numAtomsNBPad are read. */
+typedef struct {
+  int patchID;
+  int bufferOffset;        /* first atom of the patch in the per-atom arrays */
+  int bufferOffsetNBPad;   /* first nonbonded slot of the patch (multiple of 32) */
+  int numAtoms;
+  int numAtomsNBPad;       /* numAtoms rounded up to a multiple of 32 */
+  int isProxy;
+  int numPeerRecord;
+  int peerRecordStartIndex;
+  int bufferOffsetOld;
+  int numMigrationGroups;
+  int numAtomsNew;
+  int numAtomsLocal;
+  int inlinePeers[20];     /* CudaPeerRecord[5]; not read */
+} nbk_local_record;
+
+typedef struct { double x, y, z; } nbk_double3;
+
+/* Largest patch nbk_sort_patch_atoms orders (atoms per patch). */
+#define NBK_MAX_PATCH_ATOMS 2048
+
+/* Patch sort: the nonbonded order of every patch's atoms, recursive
+ * bisection of the patch at multiples of 32, then 16, then 8 atoms along the
+ * longest extent of each part, ties broken by global atom id (the atom order
+ * of src/SortAtoms.C:45-133 that the reference's host caller produces; on the
+ * GPU-resident path the reference sorts in src/MigrationCUDAKernel.cu:103-460).
+ * The atom sets of every 8-atom block (hence of every 32-atom tile) are those
+ * of the host order nbk_pack builds; within a block the atoms are in (coordinate,
+ * id) order. Writes d_sortOrder[bufferOffset + i] = the index within the patch
+ * (0..numAtoms-1) of the atom placed in the patch's nonbonded slot i.
+ * maxPatchAtoms: an upper bound of numAtoms over the patches (at most
+ * NBK_MAX_PATCH_ATOMS). d_status (may be NULL): a device int that is
+ * incremented for every patch larger than the bound (such a patch keeps its
+ * buffer order). */
+NBK_API int nbk_sort_patch_atoms(int numPatches, const nbk_local_record* d_localRecords,
+                                 int maxPatchAtoms, const double* d_pos_x, const double* d_pos_y,
+                                 const double* d_pos_z, const int* d_id, int* d_sortOrder,
+                                 int* d_status, void* stream);
+
+/* The nonbonded part of setComputePositionsKernel, src/SequencerCUDAKernel.cu:
+ * 1950-2041: xyzq[slot] = (x - centre, q * chargeScaling) with the patch centre
+ * unscaled from fractional coordinates (o + a sx + b sy + c sz, FP64) and the
+ * difference rounded once to FP32; the slots past numAtoms repeat the last
+ * atom. lattice: a, b, c, origin as 12 doubles (host). d_charge: FP32 charges
+ * (the product with chargeScaling is formed in FP64, as the reference does). */
+NBK_API int nbk_set_compute_positions(int numPatches, const nbk_local_record* d_localRecords,
+                                      const nbk_double3* d_patchCenter, const double* lattice,
+                                      const int* d_sortOrder, double chargeScaling,
+                                      const double* d_pos_x, const double* d_pos_y,
+                                      const double* d_pos_z, const float* d_charge,
+                                      nbk_float4* d_xyzq, void* stream);
+
+/* CudaComputeNonbondedKernel::setExclusionsByAtom, src/CudaComputeNonbondedKernel.cu:
+ * 3640-3645: per global atom id, (maxdiff, base) of its exclusion list in the
+ * bit array bound by nbk_bind_exclusions (host array, copied; synchronises). */
+NBK_API int nbk_set_exclusions_by_atom(nbk_handle h, int numAtoms,
+                                       const nbk_int2* h_exclusionsByAtom);
+
+/* CudaComputeNonbondedKernel::updateVdwTypesExclOnGPU, src/CudaComputeNonbondedKernel.cu:
+ * 3648-3724: the handle's per-slot vdW types, global atom indices and
+ * (base, maxdiff) exclusion indices from per-atom arrays in buffer order
+ * through d_sortOrder, as nbk_update_vdw_types_excl does from host arrays.
+ * Unlike the reference kernel, the padding slots repeat the patch's last atom.
+ * A vdW type outside the LJ table or an id outside the nbk_set_exclusions_by_atom
+ * range is written as type 0 / no exclusions and counted in d_status (a device
+ * int, may be NULL). */
+NBK_API int nbk_update_vdw_types_excl_device(nbk_handle h, int numPatches, int atomStorageSize,
+                                             const nbk_local_record* d_localRecords,
+                                             const int* d_vdwTypes, const int* d_id,
+                                             const int* d_sortOrder, int* d_status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,7 @@ static_assert(sizeof(nbk_patch_record) == 16, "CudaPatchRecord (with patchID) is
 static_assert(sizeof(nbk_tile_excl) == 128, "TileExcl is 128 bytes");
 static_assert(sizeof(nbk_exclusion) == 32, "CudaExclusion is 32 bytes");
 static_assert(sizeof(nbk_virial_energy) == sizeof(double) * 31, "VirialEnergy is 31 doubles");
+static_assert(sizeof(nbk_local_record) == 128, "CudaLocalRecord is 128 bytes");
 
 namespace {
 
@@ -82,6 +83,8 @@ struct nbk_context {
   int numComputes = 0;
   DBuf<int> vdwTypes, atomIndex;
   DBuf<int2> exclIndexMaxDiff;
+  DBuf<int2> exclByAtom;  // GPU-resident marshaling: (maxdiff, base) per global atom id
+  int numExclByAtom = 0;
   int atomDataSize = 0;
   // positions
   DBuf<float4> xyzqOwn;
@@ -297,6 +300,8 @@ int bindPositions(nbk_handle h, const nbk_float4* xyzq, int onDevice, int n, cud
 
 }  // namespace
 
+int nbk::setLastError(int code, const std::string& msg) { return setErr(code, msg); }
+
 extern "C" {
 
 NBK_API const char* nbk_last_error(void) { return g_err.c_str(); }
@@ -376,6 +381,7 @@ NBK_API int nbk_destroy(nbk_handle h) {
   h->vdwTypes.release();
   h->atomIndex.release();
   h->exclIndexMaxDiff.release();
+  h->exclByAtom.release();
   h->xyzqOwn.release();
   h->patches.release();
   h->seeds.release();
@@ -1126,5 +1132,41 @@ NBK_API int nbk_set_tuning(nbk_handle h, unsigned flags, int minBlocksPerSM, int
   h->tuneMinBlocks[key] = minBlocksPerSM;
   h->tuneSplitLog2[key] = sl;
   h->tuneMs[key] = 0.f;
+  return NBK_OK;
+}
+
+// ---- GPU-resident input marshaling -----------------------------------------
+
+NBK_API int nbk_set_exclusions_by_atom(nbk_handle h, int numAtoms, const nbk_int2* hx) {
+  int rc = checkHandle(h, "nbk_set_exclusions_by_atom");
+  if (rc) return rc;
+  if (numAtoms <= 0 || !hx) return setErr(NBK_ERR_ARG, "nbk_set_exclusions_by_atom: bad argument");
+  NBK_CUDA(h->exclByAtom.ensure(numAtoms), "nbk_set_exclusions_by_atom");
+  NBK_CUDA(cudaMemcpy(h->exclByAtom.p, hx, sizeof(int2) * numAtoms, cudaMemcpyHostToDevice),
+           "nbk_set_exclusions_by_atom");
+  h->numExclByAtom = numAtoms;
+  return NBK_OK;
+}
+
+NBK_API int nbk_update_vdw_types_excl_device(nbk_handle h, int numPatches, int n,
+                                             const nbk_local_record* rec, const int* vdw,
+                                             const int* id, const int* sortOrder, int* status,
+                                             void* stream) {
+  int rc = checkHandle(h, "nbk_update_vdw_types_excl_device");
+  if (rc) return rc;
+  if (numPatches < 0 || n <= 0 || (n & 31) || (numPatches && (!rec || !vdw || !id || !sortOrder)))
+    return setErr(NBK_ERR_ARG, "nbk_update_vdw_types_excl_device: bad argument (size must be a "
+                               "positive multiple of 32)");
+  if (!h->numExclByAtom)
+    return setErr(NBK_ERR_STATE, "nbk_update_vdw_types_excl_device: nbk_set_exclusions_by_atom first");
+  cudaStream_t st = (cudaStream_t)stream;
+  NBK_CUDA(h->vdwTypes.ensure(n), "nbk_update_vdw_types_excl_device");
+  NBK_CUDA(h->atomIndex.ensure(n), "nbk_update_vdw_types_excl_device");
+  NBK_CUDA(h->exclIndexMaxDiff.ensure(n), "nbk_update_vdw_types_excl_device");
+  NBK_CUDA(launchUpdateVdwTypesExclDevice(numPatches, rec, vdw, id, sortOrder, h->exclByAtom.p,
+                                          h->numExclByAtom, h->ljDim, n, h->vdwTypes.p,
+                                          h->atomIndex.p, h->exclIndexMaxDiff.p, status, st),
+           "nbk_update_vdw_types_excl_device");
+  h->atomDataSize = n;
   return NBK_OK;
 }

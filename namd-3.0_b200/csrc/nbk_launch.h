@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "nbk_internal.cuh"
 
 namespace nbk {
@@ -90,5 +92,16 @@ struct AdjArgs {
 };
 cudaError_t launchAdjoint(const AdjArgs& a, bool doSlow, int numSM, int n, float4* out,
                           cudaStream_t st);
+
+// Sets the message nbk_last_error returns on this thread; returns code.
+int setLastError(int code, const std::string& msg);
+
+// Per-slot vdW types, atom indices and exclusion indices from per-atom arrays
+// in buffer order (GPU-resident marshaling, nbk_resident.cu).
+cudaError_t launchUpdateVdwTypesExclDevice(int numPatches, const nbk_local_record* rec,
+                                           const int* vdw, const int* gid, const int* sortOrder,
+                                           const int2* exclByAtom, int numExclAtoms, int ljDim,
+                                           int storage, int* vdwTypes, int* atomIndex, int2* excl,
+                                           int* status, cudaStream_t st);
 
 }  // namespace nbk

@@ -263,6 +263,7 @@ class Packed:
             h = C.c_void_p()
             _hcheck(lib.nbk_pack(system._h, patch_dim, coulomb_scaling, C.byref(h)), "nbk_pack")
             self.systems = [system]
+            self.coulomb_scaling = coulomb_scaling
         else:
             h = _handle
             self.systems = list(_systems)
@@ -276,7 +277,9 @@ class Packed:
         h = C.c_void_p()
         _hcheck(host_lib().nbk_pack_many(arr, len(systems), patch_dim, coulomb_scaling,
                                          C.byref(h)), "nbk_pack_many")
-        return cls(None, _handle=h, _systems=systems)
+        out = cls(None, _handle=h, _systems=systems)
+        out.coulomb_scaling = coulomb_scaling
+        return out
 
     def __del__(self):
         if getattr(self, "_h", None) and _host is not None:
@@ -361,6 +364,11 @@ def dev_lib() -> C.CDLL:
                                     vp, vp]
         lib.nbk_reduce_virial_energy_batch.argtypes = [vp, u, vp, i, vp]
         lib.nbk_get_pair_counts.argtypes = [vp, C.POINTER(C.c_longlong), i, vp]
+        lib.nbk_sort_patch_atoms.argtypes = [i, vp, i, vp, vp, vp, vp, vp, vp, vp]
+        lib.nbk_set_compute_positions.argtypes = [i, vp, vp, C.POINTER(C.c_double), vp,
+                                                  C.c_double, vp, vp, vp, vp, vp, vp]
+        lib.nbk_set_exclusions_by_atom.argtypes = [vp, i, vp]
+        lib.nbk_update_vdw_types_excl_device.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp]
         _dev = lib
     return _dev
 
@@ -564,6 +572,22 @@ class Nonbonded:
                 "nbk_get_tuning")
         return {"ctas_per_sm": b.value, "warps_per_list": sp.value, "ms": ms.value}
 
+    # -- GPU-resident input marshaling --------------------------------------
+    def set_exclusions_by_atom(self, excl_by_atom):
+        """(maxdiff, base) per global atom id, int32 [natoms, 2] (host)."""
+        a = np.ascontiguousarray(excl_by_atom, dtype=np.int32)
+        _dcheck(dev_lib().nbk_set_exclusions_by_atom(self._h, len(a), a.ctypes.data),
+                "nbk_set_exclusions_by_atom")
+
+    def update_vdw_types_excl_device(self, layout, sort_order, status=None, stream=None):
+        """Per-slot vdW types / atom indices / exclusion indices from the
+        device-resident per-atom arrays of a ResidentLayout."""
+        d = layout.dev
+        _dcheck(dev_lib().nbk_update_vdw_types_excl_device(
+            self._h, layout.numPatches, layout.atomStorageSize, _ptr(d["records"]),
+            _ptr(d["vdw"]), _ptr(d["id"]), _ptr(sort_order), _ptr(status), stream),
+            "nbk_update_vdw_types_excl_device")
+
     def export_tile_lists(self, stream=None):
         nl, nj = C.c_int(0), C.c_int(0)
         L = dev_lib()
@@ -604,3 +628,94 @@ def pairs_from_tile_lists(tl, jatom, excl, storage):
     k = np.concatenate(keys)
     k.sort()
     return k
+
+
+# ---------------------------------------------------------------------------
+# GPU-resident input marshaling
+# ---------------------------------------------------------------------------
+LOCAL_RECORD_WORDS = 32   # nbk_local_record (CudaLocalRecord) is 128 bytes
+
+
+class ResidentLayout:
+    """The per-atom arrays a GPU-resident integrator holds for one system, in
+    buffer order (patch by patch, each patch's atoms in ascending global id or
+    in the order `order_in_patch` gives), with the CudaLocalRecord of every
+    patch -- built from a System and its Packed layout, on the host and as
+    device tensors (`dev`). Patch assignment and slot ranges are the Packed
+    layout's."""
+
+    def __init__(self, system: System, packed: Packed, device=0, shuffle_seed=None):
+        """device=None builds the host arrays only."""
+        import torch
+        a = system.arrays()
+        n = system.natoms
+        pa = packed.patches                       # numAtoms, numFreeAtoms, atomStart, id
+        slot = packed.slotOfAtom
+        start = pa[:, 2]
+        patch_of = np.searchsorted(start, slot, side="right") - 1
+        ids = np.lexsort((np.arange(n), patch_of))  # by patch, then by id
+        if shuffle_seed is not None:
+            rng = np.random.default_rng(shuffle_seed)
+            off = 0
+            for p in range(len(pa)):
+                k = int(pa[p, 0])
+                rng.shuffle(ids[off:off + k])
+                off += k
+        self.numPatches = len(pa)
+        self.atomStorageSize = packed.atomStorageSize
+        self.ids = ids.astype(np.int32)            # global id at each buffer position
+        rec = np.zeros((len(pa), LOCAL_RECORD_WORDS), dtype=np.int32)
+        counts = pa[:, 0]
+        rec[:, 0] = np.arange(len(pa))
+        rec[:, 1] = np.concatenate([[0], np.cumsum(counts)[:-1]])
+        rec[:, 2] = start
+        rec[:, 3] = counts
+        rec[:, 4] = ((counts + 31) // 32) * 32
+        self.records = rec
+        pos = np.asarray(a["pos"], dtype=np.float64).reshape(-1, 3)
+        self.pos = np.ascontiguousarray(pos[ids].T)              # [3, natoms]
+        self.charge = np.asarray(a["charge"], dtype=np.float32)[ids]
+        self.vdw = np.asarray(a["type"], dtype=np.int32)[ids]
+        em = packed.exclIndexMaxDiff[slot]                      # (base, maxdiff) per atom id
+        self.excl_by_atom = np.ascontiguousarray(em[:, ::-1], dtype=np.int32)
+        # patch centres as fractional coordinates of an identity lattice
+        # (so that the unscaled centre is exactly the Cartesian one)
+        self.centres = np.ascontiguousarray(packed.patchCenter, dtype=np.float64)
+        self.lattice = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], dtype=np.float64)
+        self.qscale = float(np.sqrt(332.0636 * packed.coulomb_scaling))
+        self.dev = None
+        if device is None:
+            return
+        dev = torch.device("cuda", device)
+        t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        self.dev = {"records": t(rec), "x": t(self.pos[0]), "y": t(self.pos[1]),
+                    "z": t(self.pos[2]), "charge": t(self.charge), "vdw": t(self.vdw),
+                    "id": t(self.ids), "centres": t(self.centres)}
+
+    def host_sort_order(self, packed: Packed):
+        """The sort order that reproduces the Packed slot order exactly."""
+        order = np.zeros(len(self.ids), dtype=np.int32)
+        slot = packed.slotOfAtom[self.ids]
+        for p in range(self.numPatches):
+            b, k = self.records[p, 1], self.records[p, 3]
+            if k == 0:
+                continue
+            local = slot[b:b + k] - self.records[p, 2]           # slot within patch
+            order[b + local] = np.arange(k, dtype=np.int32)
+        return order
+
+    def sort_patch_atoms(self, sort_order, max_patch_atoms=None, status=None, stream=None):
+        d = self.dev
+        m = int(self.records[:, 3].max()) if max_patch_atoms is None else max_patch_atoms
+        _dcheck(dev_lib().nbk_sort_patch_atoms(self.numPatches, _ptr(d["records"]), m,
+                                               _ptr(d["x"]), _ptr(d["y"]), _ptr(d["z"]),
+                                               _ptr(d["id"]), _ptr(sort_order), _ptr(status),
+                                               stream), "nbk_sort_patch_atoms")
+
+    def set_compute_positions(self, sort_order, xyzq, stream=None):
+        d = self.dev
+        lat = self.lattice.ctypes.data_as(C.POINTER(C.c_double))
+        _dcheck(dev_lib().nbk_set_compute_positions(
+            self.numPatches, _ptr(d["records"]), _ptr(d["centres"]), lat, _ptr(sort_order),
+            self.qscale, _ptr(d["x"]), _ptr(d["y"]), _ptr(d["z"]), _ptr(d["charge"]),
+            _ptr(xyzq), stream), "nbk_set_compute_positions")
