@@ -68,6 +68,13 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
   // folded in at the end of every j tile, so that the sums do not depend on
   // how a list's tiles are split among warps
   __shared__ long long s_fi[kForceWarps][6][kWarp];
+  // FP32 mode: each lane's energies of the current list part in fixed point
+  // (s_eq) and of the current tile group in FP32 (s_eg), and the warp's
+  // fixed-point energy totals (s_acc, lane 0), kept in shared memory rather
+  // than in registers the pair loop needs
+  __shared__ long long s_eq[kForceWarps][3][kWarp];
+  __shared__ float s_eg[kForceWarps][3][kWarp];
+  __shared__ long long s_acc[kForceWarps][3];
 
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -87,6 +94,12 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
   if (!doE64) {
 #pragma unroll
     for (int q = 0; q < 6; ++q) s_fi[wib][q][lane] = 0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      s_eq[wib][q][lane] = 0;
+      s_eg[wib][q][lane] = 0.f;
+    }
+    if (lane < 3) s_acc[wib][lane] = 0;
   }  // interacting pairs seen by this lane (energy evaluations)
   int curRep = 0;  // replica whose accumulators the warp is holding
 
@@ -111,6 +124,12 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     if (doBatch) {
       const int rep = __ldg(&a.compRep[tl.icompute]);
       if (rep != curRep) {
+        if (!doE64 && lane == 0) {
+          accE0 = s_acc[wib][0];
+          accE1 = s_acc[wib][1];
+          accE2 = s_acc[wib][2];
+          s_acc[wib][0] = s_acc[wib][1] = s_acc[wib][2] = 0;
+        }
         flushWarp<doEnergy, doVirial>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1,
                                       accE2, accVir, npair);
         curRep = rep;
@@ -144,8 +163,6 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
     float2 fisx2 = f2(0.f), fisy2 = f2(0.f), fisz2 = f2(0.f);
     double eV = 0.0, eE = 0.0, eS = 0.0;         // FP64 energy mode, per list
-    long long eVq = 0, eEq = 0, eSq = 0;         // FP32 mode, fixed point per tile group
-    float eVg = 0.f, eEg = 0.f, eSg = 0.f;       // FP32 mode, the current tile group
     double wv[6] = {0, 0, 0, 0, 0, 0}, ws[6] = {0, 0, 0, 0, 0, 0};  // FP64 pair virials
 
     for (int jt = jtFirst; jt <= jtLast; ++jt) {
@@ -350,18 +367,20 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
         if (doE64) {
           eV += (double)eVt;
         } else {
-          eVg += eVt;
-          eEg += eEt;
-          if (doSlow) eSg += eSt;
+          s_eg[wib][0][lane] += eVt;
+          s_eg[wib][1][lane] += eEt;
+          if (doSlow) s_eg[wib][2][lane] += eSt;
         }
       }
       if (!doE64 && ((((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0) || jt == jtLast)) {
         // end of a tile group: its energies and i forces into fixed point
         if (doEnergy) {
-          eVq += toFixedEnergyF(eVg);
-          eEq += toFixedEnergyF(eEg);
-          if (doSlow) eSq += toFixedEnergyF(eSg);
-          eVg = eEg = eSg = 0.f;
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            if (q == 2 && !doSlow) break;
+            s_eq[wib][q][lane] += toFixedEnergyF(s_eg[wib][q][lane]);
+            s_eg[wib][q][lane] = 0.f;
+          }
         }
         s_fi[wib][0][lane] += (long long)toFixedForce(fix2.x + fix2.y);
         s_fi[wib][1][lane] += (long long)toFixedForce(fiy2.x + fiy2.y);
@@ -457,20 +476,32 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
         sE = toFixedEnergy(warpSumD(eE));
         if (doSlow) sS = toFixedEnergy(warpSumD(eS));
       } else {
-        sV = warpSumLL(eVq);
-        sE = warpSumLL(eEq);
-        if (doSlow) sS = warpSumLL(eSq);
+        sV = warpSumLL(s_eq[wib][0][lane]);
+        sE = warpSumLL(s_eq[wib][1][lane]);
+        if (doSlow) sS = warpSumLL(s_eq[wib][2][lane]);
+        s_eq[wib][0][lane] = s_eq[wib][1][lane] = s_eq[wib][2][lane] = 0;
       }
       if (lane == 0) {
-        accE0 += sV;
-        accE1 += sE;
-        accE2 += sS;
+        if (doE64) {
+          accE0 += sV;
+          accE1 += sE;
+          accE2 += sS;
+        } else {
+          s_acc[wib][0] += sV;
+          s_acc[wib][1] += sE;
+          s_acc[wib][2] += sS;
+        }
       }
     }
   }  // lists
 
   // per-warp flush of the fixed-point accumulators (no block barrier, so a
   // warp that runs out of lists retires at once)
+  if (!doE64 && lane == 0) {
+    accE0 = s_acc[wib][0];
+    accE1 = s_acc[wib][1];
+    accE2 = s_acc[wib][2];
+  }
   flushWarp<doEnergy, doVirial>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1, accE2,
                                 accVir, npair);
 }
