@@ -48,8 +48,8 @@ __device__ __forceinline__ int splitPoint(int begin, int end) {
   return split;
 }
 
-// One block per patch. Shared memory (dynamic): x, y, z (double) and id, ord,
-// tmp (int) per atom for maxN atoms.
+// One block per patch. Shared memory (dynamic) per atom for maxN atoms: x, y,
+// z and the current sort key (double), id, ord, tmp and the key's id (int).
 __global__ void __launch_bounds__(kSortThreads)
     sortPatchAtomsKernel(int numPatches, const nbk_local_record* __restrict__ rec, int maxN,
                          const double* __restrict__ px, const double* __restrict__ py,
@@ -59,9 +59,11 @@ __global__ void __launch_bounds__(kSortThreads)
   double* s_x = s_dyn;
   double* s_y = s_x + maxN;
   double* s_z = s_y + maxN;
-  int* s_id = reinterpret_cast<int*>(s_z + maxN);
+  double* s_key = s_z + maxN;  // by position: the coordinate the position's part is split on
+  int* s_id = reinterpret_cast<int*>(s_key + maxN);
   int* s_ord = s_id + maxN;
   int* s_tmp = s_ord + maxN;
+  int* s_kid = s_tmp + maxN;   // by position: the atom id (tie break)
   __shared__ int s_rb[kMaxRanges], s_re[kMaxRanges], s_rs[kMaxRanges], s_ax[kMaxRanges];
   __shared__ int s_split[kMaxRanges / 2];
   __shared__ int s_numRanges, s_numNext;
@@ -122,22 +124,32 @@ __global__ void __launch_bounds__(kSortThreads)
         }
       }
       __syncthreads();
-      // rank every atom of a split part by (coordinate on the part's axis, id)
+      // the split key of every position of a split part, stored by position so
+      // that the ranking reads it without indirection
       for (int r = 0; r < nr; ++r) {
         const int b = s_rb[r], e = s_re[r];
         if (s_rs[r] < 0) continue;
         const double* key = s_ax[r] == 0 ? s_x : (s_ax[r] == 1 ? s_y : s_z);
         for (int k = b + threadIdx.x; k < e; k += blockDim.x) {
           const int a = s_ord[k];
-          const double ka = key[a];
-          const int ia = s_id[a];
+          s_key[k] = key[a];
+          s_kid[k] = s_id[a];
+        }
+      }
+      __syncthreads();
+      // rank every atom of a split part by (coordinate on the part's axis, id)
+      for (int r = 0; r < nr; ++r) {
+        const int b = s_rb[r], e = s_re[r];
+        if (s_rs[r] < 0) continue;
+        for (int k = b + threadIdx.x; k < e; k += blockDim.x) {
+          const double ka = s_key[k];
+          const int ia = s_kid[k];
           int rank = 0;
           for (int m = b; m < e; ++m) {
-            const int c = s_ord[m];
-            const double kc = key[c];
-            rank += (kc < ka || (kc == ka && s_id[c] < ia)) ? 1 : 0;
+            const double kc = s_key[m];
+            rank += (kc < ka || (kc == ka && s_kid[m] < ia)) ? 1 : 0;
           }
-          s_tmp[b + rank] = a;
+          s_tmp[b + rank] = s_ord[k];
         }
       }
       __syncthreads();
@@ -267,7 +279,7 @@ extern "C" NBK_API int nbk_sort_patch_atoms(int numPatches, const nbk_local_reco
     return setLastError(NBK_ERR_ARG, "nbk_sort_patch_atoms: maxPatchAtoms must be in 1.." +
                                          std::to_string(NBK_MAX_PATCH_ATOMS));
   if (numPatches == 0) return NBK_OK;
-  const size_t smem = (size_t)maxPatchAtoms * (3 * sizeof(double) + 3 * sizeof(int));
+  const size_t smem = (size_t)maxPatchAtoms * (4 * sizeof(double) + 4 * sizeof(int));
   cudaError_t e = cudaFuncSetAttribute(sortPatchAtomsKernel,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess) {
