@@ -44,3 +44,16 @@ def test_autotune_keeps_a_timed_shape():
     assert np.array_equal(X1, X2)
     assert r1["energyVdw"] == r2["energyVdw"]
     print("autotuned shape", t)
+
+
+def test_launch_sequence_per_register_cap():
+    """One pairlist evaluation, then one steady evaluation at 4, 5 and 6 CTAs
+    per SM (one warp per tile list) on the 20,000-atom mixed system: the fixed
+    launch sequence of the per-register-cap kernel profiles."""
+    p = nbk.Packed(mixed_box(natoms=20000))
+    run = GpuRun(p)
+    run.build()
+    run.eval(ALL | nbk.NBK_PAIRLIST)
+    for b in (4, 5, 6):
+        run.nb.set_tuning(ALL, b, 1)
+        run.eval(ALL)
