@@ -219,6 +219,7 @@ def resident_timing(sys_, packed, local_rank, stream, reps=20):
     for name, fn in calls.items():
         fn()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda._sleep(50_000_000)   # keeps the GPU busy while the host enqueues the reps
         a.record(stream)
         for _ in range(reps):
             fn()
@@ -233,6 +234,75 @@ def resident_timing(sys_, packed, local_rank, stream, reps=20):
     out["patches"] = int(lay.numPatches)
     out["max_patch_atoms"] = int(lay.records[:, 3].max())
     return out
+
+
+def pme_timing(sys_, local_rank, stream, reps=20):
+    """PME reciprocal space for the same atoms (nbk_pme_*): grid ~1 A (FFT-friendly
+    sizes), B-spline order 4, the short-range path's Ewald coefficient; each
+    phase timed with CUDA events (mean of `reps`), energy + virial on."""
+    import torch
+    import nbk
+    dev = torch.device("cuda", local_rank)
+    st = stream.cuda_stream
+    a = sys_.arrays()
+    box = np.asarray(a["box"], dtype=np.float64)
+    K = [next(k for k in range(int(np.ceil(b)), 4 * int(np.ceil(b)) + 8)
+              if all(f in (2, 3, 5) for f in _factors(k))) for b in box]
+    L = np.diag(box)
+    pos = np.asarray(a["pos"], dtype=np.float64).reshape(-1, 3)
+    n = len(pos)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    x, y, z = t(pos[:, 0]), t(pos[:, 1]), t(pos[:, 2])
+    q = t(np.asarray(a["charge"], dtype=np.float32))
+    atoms = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    force = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+    params = nbk.NonbondedParams()
+    p = nbk.Pme(K, 4, params.ewaldcof, local_rank)
+    lat12 = np.concatenate([L.reshape(-1), np.zeros(3)])
+    conv = lambda: nbk.Pme.atoms_from_positions(x, y, z, q, np.sqrt(332.0636), lat12, atoms,
+                                                stream=st)
+    phases = [("spread_us", lambda: p.spread(atoms, n, st)),
+              ("fft_solve_fft_us", lambda: p.solve(L, nbk.NBK_ENERGY | nbk.NBK_VIRIAL, st)),
+              ("gather_us", lambda: p.gather(atoms, n, L, force, st))]
+    out = {"grid": K, "order": 4, "atoms": n}
+    conv()
+    for _, fn in phases:
+        fn()
+    # the host enqueues every launch while the GPU sleeps, so the events time
+    # the kernels back to back rather than the host's launch overhead
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(1 + (1 + len(phases)) * reps)]
+    torch.cuda._sleep(50_000_000)
+    ev[0].record(stream)
+    k = 1
+    for _ in range(reps):
+        conv()
+        ev[k].record(stream)
+        k += 1
+        for _, fn in phases:
+            fn()
+            ev[k].record(stream)
+            k += 1
+    torch.cuda.synchronize(dev)
+    names = ["atoms_us"] + [nm for nm, _ in phases]
+    for j, nm in enumerate(names):
+        out[nm] = sum(ev[r * len(names) + j].elapsed_time(ev[r * len(names) + j + 1])
+                      for r in range(reps)) * 1e3 / reps
+    out["total_us"] = out["spread_us"] + out["fft_solve_fft_us"] + out["gather_us"]
+    out["energy"] = p.energy_virial(st)[0]
+    p.close()
+    return out
+
+
+def _factors(k):
+    f, d = [], 2
+    while d * d <= k:
+        while k % d == 0:
+            f.append(d)
+            k //= d
+        d += 1
+    if k > 1:
+        f.append(k)
+    return f
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -376,6 +446,7 @@ def run_gpu(args, rank, world, local_rank):
            "d2h_bytes_per_step": 2 * 16 * n + 8 * 31, "steps": ke}
 
     resident = resident_timing(sys_, packed, local_rank, stream)
+    pme_t = pme_timing(sys_, local_rank, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -396,6 +467,7 @@ def run_gpu(args, rank, world, local_rank):
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks,
             "resident_marshaling": resident,
+            "pme_reciprocal": pme_t,
             "wall_s_timed_region": wall,
         }
         print(json.dumps(out))

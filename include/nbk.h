@@ -416,6 +416,69 @@ NBK_API int nbk_set_compute_positions(int numPatches, const nbk_local_record* d_
                                       const double* d_pos_z, const float* d_charge,
                                       nbk_float4* d_xyzq, void* stream);
 
+/* ---- PME reciprocal space -------------------------------------------------------
+ * The long-range half of the slow (PME) forces that the short-range kernel's
+ * slow buffers hold the real-space half of: smooth particle-mesh Ewald on one
+ * GPU, the single-device path of CudaPmeRealSpaceCompute /
+ * CudaPmeKSpaceCompute / CudaFFTCompute (src/CudaPmeSolverUtil.h:60-160,
+ * src/CudaPmeSolverUtilKernel.cu). Atoms are CudaAtom records holding
+ * fractional coordinates in [0, 1) and scaled charges, as ComputePmeCUDA
+ * sends them (src/ComputePmeCUDA.C:281-300). Charges are spread with the
+ * reference's B-spline order and grid-offset convention into a 64-bit
+ * fixed-point grid (deterministic: integer sums do not depend on the order of
+ * the atomics), transformed with cuFFT (real-to-complex, x fastest), scaled by
+ * the influence function with the reference's B-spline moduli, transformed
+ * back and interpolated to forces. Not thread-safe per handle. */
+typedef struct nbk_pme_s* nbk_pme;
+
+/* PmeGrid (src/PmeBase.h): grid points per lattice vector and B-spline
+ * order (4, 6 or 8). */
+typedef struct {
+  int K1, K2, K3;
+  int order;
+} nbk_pme_grid;
+
+NBK_API int nbk_pme_create(int deviceID, const nbk_pme_grid* grid, double ewaldcof, nbk_pme* out);
+NBK_API int nbk_pme_destroy(nbk_pme pme);
+
+/* ComputePmeCUDA::sendAtoms' conversion (src/ComputePmeCUDA.C:281-300) on the
+ * device: w = r . a_r shifted into [0, 1) by w - (floor(w + 1/2) - 1/2), in
+ * FP64, rounded to FP32 (a value rounded up to 1 becomes 0); q = charge *
+ * chargeScaling in FP64. lattice: a, b, c, origin (12 doubles, host). */
+NBK_API int nbk_pme_atoms_from_positions(int numAtoms, const double* d_x, const double* d_y,
+                                         const double* d_z, const float* d_charge,
+                                         double chargeScaling, const double* lattice,
+                                         nbk_float4* d_atoms, void* stream);
+
+/* CudaPmeRealSpaceCompute::copyAtoms + spreadCharge (src/CudaPmeSolverUtil.C,
+ * spread_charge_kernel src/CudaPmeSolverUtilKernel.cu:427-530). */
+NBK_API int nbk_pme_spread_charge(nbk_pme pme, int numAtoms, const nbk_float4* d_atoms,
+                                  void* stream);
+
+/* CudaFFTCompute::forward, CudaPmeKSpaceCompute::solve (scalar_sum_kernel,
+ * src/CudaPmeSolverUtilKernel.cu:74-325) and CudaFFTCompute::backward.
+ * lattice: a, b, c (9 doubles, host). flags: NBK_ENERGY and/or NBK_VIRIAL.
+ * Consumes the charge grid of the last nbk_pme_spread_charge: afterwards the
+ * grid holds the potential that nbk_pme_gather_force interpolates, so every
+ * solve needs a spread before it. */
+NBK_API int nbk_pme_solve(nbk_pme pme, const double* lattice, unsigned flags, void* stream);
+
+/* CudaPmeRealSpaceCompute::gatherForce (gather_force,
+ * src/CudaPmeSolverUtilKernel.cu:708-945) followed by ComputePmeCUDA's
+ * conversion to Cartesian forces (src/ComputePmeCUDA.C:640-652):
+ * d_force[i] = f1 a_r + f2 b_r + f3 c_r. lattice: a, b, c (9 doubles, host). */
+NBK_API int nbk_pme_gather_force(nbk_pme pme, int numAtoms, const nbk_float4* d_atoms,
+                                 const double* lattice, nbk_float3* d_force, void* stream);
+
+/* CudaPmeKSpaceCompute::getEnergy / getVirial of the last nbk_pme_solve
+ * (synchronises). virial: 9 doubles, row-major, sum of r (x) F convention. */
+NBK_API int nbk_pme_get_energy_virial(nbk_pme pme, double* energy, double* virial, void* stream);
+
+/* The Ewald self energy -beta/sqrt(pi) sum q^2 (selfEnergyKernel,
+ * src/CudaPmeSolverUtilKernel.cu:1192-1216; synchronises). */
+NBK_API int nbk_pme_self_energy(nbk_pme pme, int numAtoms, const nbk_float4* d_atoms,
+                                double* selfEnergy, void* stream);
+
 /* CudaComputeNonbondedKernel::setExclusionsByAtom, src/CudaComputeNonbondedKernel.cu:
  * 3640-3645: per global atom id, (maxdiff, base) of its exclusion list in the
  * bit array bound by nbk_bind_exclusions (host array, copied; synchronises). */

@@ -369,8 +369,21 @@ def dev_lib() -> C.CDLL:
                                                   C.c_double, vp, vp, vp, vp, vp, vp]
         lib.nbk_set_exclusions_by_atom.argtypes = [vp, i, vp]
         lib.nbk_update_vdw_types_excl_device.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp]
+        dp = C.POINTER(C.c_double)
+        lib.nbk_pme_create.argtypes = [i, C.POINTER(PmeGrid), C.c_double, C.POINTER(vp)]
+        lib.nbk_pme_destroy.argtypes = [vp]
+        lib.nbk_pme_atoms_from_positions.argtypes = [i, vp, vp, vp, vp, C.c_double, dp, vp, vp]
+        lib.nbk_pme_spread_charge.argtypes = [vp, i, vp, vp]
+        lib.nbk_pme_solve.argtypes = [vp, dp, u, vp]
+        lib.nbk_pme_gather_force.argtypes = [vp, i, vp, dp, vp, vp]
+        lib.nbk_pme_get_energy_virial.argtypes = [vp, dp, dp, vp]
+        lib.nbk_pme_self_energy.argtypes = [vp, i, vp, dp, vp]
         _dev = lib
     return _dev
+
+
+class PmeGrid(C.Structure):
+    _fields_ = [("K1", C.c_int), ("K2", C.c_int), ("K3", C.c_int), ("order", C.c_int)]
 
 
 def _dcheck(rc: int, what: str):
@@ -719,3 +732,79 @@ class ResidentLayout:
             self.numPatches, _ptr(d["records"]), _ptr(d["centres"]), lat, _ptr(sort_order),
             self.qscale, _ptr(d["x"]), _ptr(d["y"]), _ptr(d["z"]), _ptr(d["charge"]),
             _ptr(xyzq), stream), "nbk_set_compute_positions")
+
+
+# ---------------------------------------------------------------------------
+# PME reciprocal space
+# ---------------------------------------------------------------------------
+def _lat(lattice, n):
+    a = np.ascontiguousarray(np.asarray(lattice, dtype=np.float64).reshape(-1)[:n])
+    assert a.size == n
+    return a
+
+
+class Pme:
+    """PME reciprocal space on one GPU (nbk_pme_*): grid (K1, K2, K3), B-spline
+    order 4, 6 or 8, Ewald coefficient ewaldcof. Atoms are device float4
+    (fractional x, y, z in [0, 1), scaled charge); lattices are (a, b, c)."""
+
+    def __init__(self, K, order, ewaldcof, device=0):
+        g = PmeGrid(int(K[0]), int(K[1]), int(K[2]), int(order))
+        h = C.c_void_p()
+        _dcheck(dev_lib().nbk_pme_create(device, C.byref(g), float(ewaldcof), C.byref(h)),
+                "nbk_pme_create")
+        self._h = h
+        self.K = tuple(int(k) for k in K)
+        self.order = int(order)
+        self.ewaldcof = float(ewaldcof)
+
+    def close(self):
+        if getattr(self, "_h", None) and _dev is not None:
+            _dev.nbk_pme_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    @staticmethod
+    def atoms_from_positions(x, y, z, charge, qscale, lattice_abco, atoms, stream=None):
+        """Device FP64 positions and FP32 charges -> fractional float4 atoms."""
+        lat = _lat(lattice_abco, 12)
+        n = int(x.numel()) if hasattr(x, "numel") else len(x)
+        _dcheck(dev_lib().nbk_pme_atoms_from_positions(
+            n, _ptr(x), _ptr(y), _ptr(z), _ptr(charge), float(qscale),
+            lat.ctypes.data_as(C.POINTER(C.c_double)), _ptr(atoms), stream),
+            "nbk_pme_atoms_from_positions")
+
+    def spread(self, atoms, n, stream=None):
+        _dcheck(dev_lib().nbk_pme_spread_charge(self._h, int(n), _ptr(atoms), stream),
+                "nbk_pme_spread_charge")
+
+    def solve(self, lattice, flags=NBK_ENERGY | NBK_VIRIAL, stream=None):
+        lat = _lat(lattice, 9)
+        _dcheck(dev_lib().nbk_pme_solve(self._h, lat.ctypes.data_as(C.POINTER(C.c_double)),
+                                        flags, stream), "nbk_pme_solve")
+
+    def gather(self, atoms, n, lattice, force, stream=None):
+        lat = _lat(lattice, 9)
+        _dcheck(dev_lib().nbk_pme_gather_force(self._h, int(n), _ptr(atoms),
+                                               lat.ctypes.data_as(C.POINTER(C.c_double)),
+                                               _ptr(force), stream), "nbk_pme_gather_force")
+
+    def energy_virial(self, stream=None):
+        e = C.c_double(0)
+        v = (C.c_double * 9)()
+        _dcheck(dev_lib().nbk_pme_get_energy_virial(self._h, C.byref(e), v, stream),
+                "nbk_pme_get_energy_virial")
+        return float(e.value), np.array(v[:], dtype=np.float64).reshape(3, 3)
+
+    def self_energy(self, atoms, n, stream=None):
+        e = C.c_double(0)
+        _dcheck(dev_lib().nbk_pme_self_energy(self._h, int(n), _ptr(atoms), C.byref(e), stream),
+                "nbk_pme_self_energy")
+        return float(e.value)
+
+    def compute(self, atoms, n, lattice, force, flags=NBK_ENERGY | NBK_VIRIAL, stream=None):
+        """Spread, solve, gather: forces into `force` (device float3[n])."""
+        self.spread(atoms, n, stream)
+        self.solve(lattice, flags, stream)
+        self.gather(atoms, n, lattice, force, stream)
