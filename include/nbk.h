@@ -416,6 +416,31 @@ NBK_API int nbk_set_compute_positions(int numPatches, const nbk_local_record* d_
                                       const double* d_pos_z, const float* d_charge,
                                       nbk_float4* d_xyzq, void* stream);
 
+/* SequencerCUDAKernel::accumulateForceToSOA, src/SequencerCUDAKernel.cu:179-297
+ * (one device): the integrator's per-atom FP64 force arrays, in buffer order,
+ * from the 64-bit fixed-point sums of the last nbk_nonbonded_force of this
+ * handle (converted exactly, not through its float4 outputs), the PME forces
+ * and the bonded force arrays:
+ *   f_normal = f_bond
+ *   f_nbond  = nonbonded fast + f_bond_nbond
+ *   f_slow   = PME + nonbonded slow + f_bond_slow   (added in this order)
+ * maxForceNumber 0 writes f_normal only, 1 also f_nbond, 2 also f_slow (the
+ * reference's levels). d_sortOrder as nbk_sort_patch_atoms writes it (the
+ * reference takes its inverse, patchUnsortOrder). d_f_bond, d_f_bond_nbond,
+ * d_f_bond_slow: [3][forceStride] FP64 (x, y, z rows; NULL = zero). d_f_pme:
+ * Cartesian float3 per atom in buffer order (NULL = zero), e.g. from
+ * nbk_pme_gather_force on the same atoms. */
+NBK_API int nbk_accumulate_forces_to_soa(nbk_handle h, int maxForceNumber, int numPatches,
+                                         const nbk_local_record* d_localRecords,
+                                         const int* d_sortOrder, const double* d_f_bond,
+                                         const double* d_f_bond_nbond, const double* d_f_bond_slow,
+                                         int forceStride, const nbk_float3* d_f_pme,
+                                         double* d_f_normal_x, double* d_f_normal_y,
+                                         double* d_f_normal_z, double* d_f_nbond_x,
+                                         double* d_f_nbond_y, double* d_f_nbond_z,
+                                         double* d_f_slow_x, double* d_f_slow_y,
+                                         double* d_f_slow_z, void* stream);
+
 /* ---- PME reciprocal space -------------------------------------------------------
  * The long-range half of the slow (PME) forces that the short-range kernel's
  * slow buffers hold the real-space half of: smooth particle-mesh Ewald on one

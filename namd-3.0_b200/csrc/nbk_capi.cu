@@ -1170,3 +1170,44 @@ NBK_API int nbk_update_vdw_types_excl_device(nbk_handle h, int numPatches, int n
   h->atomDataSize = n;
   return NBK_OK;
 }
+
+NBK_API int nbk_accumulate_forces_to_soa(nbk_handle h, int maxForceNumber, int numPatches,
+                                         const nbk_local_record* rec, const int* sortOrder,
+                                         const double* fBond, const double* fBondNbond,
+                                         const double* fBondSlow, int forceStride,
+                                         const nbk_float3* fPme, double* nx, double* ny,
+                                         double* nz, double* bx, double* by, double* bz,
+                                         double* sx, double* sy, double* sz, void* stream) {
+  int rc = checkHandle(h, "nbk_accumulate_forces_to_soa");
+  if (rc) return rc;
+  if (maxForceNumber < 0 || maxForceNumber > 2 || numPatches < 0 ||
+      (numPatches && (!rec || !sortOrder || !nx || !ny || !nz)) ||
+      (maxForceNumber >= 1 && (!bx || !by || !bz)) || (maxForceNumber >= 2 && (!sx || !sy || !sz)) ||
+      ((fBond || fBondNbond || fBondSlow) && forceStride <= 0))
+    return setErr(NBK_ERR_ARG, "nbk_accumulate_forces_to_soa: bad argument");
+  if (!h->force.p || h->forceStride <= 0)
+    return setErr(NBK_ERR_STATE, "nbk_accumulate_forces_to_soa: no nbk_nonbonded_force evaluation yet");
+  AccumulateArgs a;
+  a.numPatches = numPatches;
+  a.maxForceNumber = maxForceNumber;
+  a.stride = h->forceStride;
+  a.forceStride = forceStride;
+  a.rec = rec;
+  a.sortOrder = sortOrder;
+  a.fixed = h->force.p;
+  a.fBond = fBond;
+  a.fBondNbond = fBondNbond;
+  a.fBondSlow = fBondSlow;
+  a.fPme = reinterpret_cast<const float3*>(fPme);
+  a.fNormal[0] = nx;
+  a.fNormal[1] = ny;
+  a.fNormal[2] = nz;
+  a.fNbond[0] = bx;
+  a.fNbond[1] = by;
+  a.fNbond[2] = bz;
+  a.fSlow[0] = sx;
+  a.fSlow[1] = sy;
+  a.fSlow[2] = sz;
+  NBK_CUDA(launchAccumulateForces(a, (cudaStream_t)stream), "nbk_accumulate_forces_to_soa");
+  return NBK_OK;
+}

@@ -93,6 +93,22 @@ struct AdjArgs {
 cudaError_t launchAdjoint(const AdjArgs& a, bool doSlow, int numSM, int n, float4* out,
                           cudaStream_t st);
 
+// Integrator force arrays from the fixed-point sums (nbk_accumulate_forces_to_soa).
+struct AccumulateArgs {
+  int numPatches, maxForceNumber, stride, forceStride;
+  const nbk_local_record* rec;
+  const int* sortOrder;
+  const long long* fixed;     // [6][stride]: fast x y z, slow x y z
+  const double* fBond;        // [3][forceStride] or NULL
+  const double* fBondNbond;
+  const double* fBondSlow;
+  const float3* fPme;         // per buffer atom or NULL
+  double* fNormal[3];
+  double* fNbond[3];
+  double* fSlow[3];
+};
+cudaError_t launchAccumulateForces(const AccumulateArgs& a, cudaStream_t st);
+
 // Sets the message nbk_last_error returns on this thread; returns code.
 int setLastError(int code, const std::string& msg);
 

@@ -251,7 +251,46 @@ __global__ void updateVdwTypesExclDeviceKernel(int numPatches, const nbk_local_r
   }
 }
 
+__global__ void accumulateForcesKernel(const __grid_constant__ AccumulateArgs a) {
+  for (int p = blockIdx.x; p < a.numPatches; p += gridDim.x) {
+    const int n = a.rec[p].numAtoms, off = a.rec[p].bufferOffset, offNB = a.rec[p].bufferOffsetNBPad;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+      const int b = off + min(max(a.sortOrder[off + k], 0), n - 1);  // buffer index of slot k
+      const size_t slot = (size_t)offNB + k;
+      double fn[3], fb[3], fs[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        fn[c] = a.fBond ? a.fBond[b + (size_t)c * a.forceStride] : 0.0;
+        fb[c] = (double)a.fixed[slot + (size_t)c * a.stride] * kForceScaleInv;
+        if (a.fBondNbond) fb[c] += a.fBondNbond[b + (size_t)c * a.forceStride];
+        fs[c] = a.fPme ? (double)(&a.fPme[b].x)[c] : 0.0;
+        fs[c] += (double)a.fixed[slot + (size_t)(3 + c) * a.stride] * kForceScaleInv;
+        if (a.fBondSlow) fs[c] += a.fBondSlow[b + (size_t)c * a.forceStride];
+      }
+      a.fNormal[0][b] = fn[0];
+      a.fNormal[1][b] = fn[1];
+      a.fNormal[2][b] = fn[2];
+      if (a.maxForceNumber >= 1) {
+        a.fNbond[0][b] = fb[0];
+        a.fNbond[1][b] = fb[1];
+        a.fNbond[2][b] = fb[2];
+      }
+      if (a.maxForceNumber >= 2) {
+        a.fSlow[0][b] = fs[0];
+        a.fSlow[1][b] = fs[1];
+        a.fSlow[2][b] = fs[2];
+      }
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t launchAccumulateForces(const AccumulateArgs& a, cudaStream_t st) {
+  if (a.numPatches <= 0) return cudaSuccess;
+  accumulateForcesKernel<<<min(a.numPatches, 65535), 256, 0, st>>>(a);
+  return cudaGetLastError();
+}
 
 cudaError_t launchUpdateVdwTypesExclDevice(int numPatches, const nbk_local_record* rec,
                                            const int* vdw, const int* gid, const int* sortOrder,

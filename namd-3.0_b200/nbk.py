@@ -369,6 +369,7 @@ def dev_lib() -> C.CDLL:
                                                   C.c_double, vp, vp, vp, vp, vp, vp]
         lib.nbk_set_exclusions_by_atom.argtypes = [vp, i, vp]
         lib.nbk_update_vdw_types_excl_device.argtypes = [vp, i, i, vp, vp, vp, vp, vp, vp]
+        lib.nbk_accumulate_forces_to_soa.argtypes = [vp, i, i, vp, vp, vp, vp, vp, i, vp] + [vp] * 9 + [vp]
         dp = C.POINTER(C.c_double)
         lib.nbk_pme_create.argtypes = [i, C.POINTER(PmeGrid), C.c_double, C.POINTER(vp)]
         lib.nbk_pme_destroy.argtypes = [vp]
@@ -600,6 +601,23 @@ class Nonbonded:
             self._h, layout.numPatches, layout.atomStorageSize, _ptr(d["records"]),
             _ptr(d["vdw"]), _ptr(d["id"]), _ptr(sort_order), _ptr(status), stream),
             "nbk_update_vdw_types_excl_device")
+
+    def accumulate_forces_to_soa(self, layout, sort_order, max_force_number, normal, nbond=None,
+                                 slow=None, f_bond=None, f_bond_nbond=None, f_bond_slow=None,
+                                 f_pme=None, stream=None):
+        """Integrator FP64 force arrays (buffer order) from the last evaluation's
+        fixed-point sums: normal, nbond, slow are [3, natoms] float64 tensors;
+        f_bond* are [3, natoms] float64 (or None), f_pme [natoms, 3] float32."""
+        d = layout.dev
+        rows = lambda t: [None] * 3 if t is None else [t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr()]
+        fs = 0
+        for t in (f_bond, f_bond_nbond, f_bond_slow):
+            if t is not None:
+                fs = int(t.stride(0))
+        _dcheck(dev_lib().nbk_accumulate_forces_to_soa(
+            self._h, int(max_force_number), layout.numPatches, _ptr(d["records"]), _ptr(sort_order),
+            _ptr(f_bond), _ptr(f_bond_nbond), _ptr(f_bond_slow), fs, _ptr(f_pme),
+            *rows(normal), *rows(nbond), *rows(slow), stream), "nbk_accumulate_forces_to_soa")
 
     def export_tile_lists(self, stream=None):
         nl, nj = C.c_int(0), C.c_int(0)

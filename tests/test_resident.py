@@ -172,3 +172,46 @@ def test_resident_pipeline_vs_oracle(system):
     assert rms_rel(F[dev_slot], Fo[host_slot]) < FORCE_RMS_TOL
     assert rms_rel(S[dev_slot], So[host_slot]) < FORCE_RMS_TOL
     assert abs(res["energyVdw"] - ro["energyVdw"]) <= ENERGY_TOL * abs(ro["energyVdw"])
+
+
+@pytest.mark.gpu
+def test_accumulate_forces_to_soa_exact(system):
+    """The integrator's FP64 force arrays from the fixed-point sums, the PME
+    forces and the bonded arrays: bit for bit the sums a host forms from the
+    exported fixed-point forces, in buffer order, at every force level."""
+    import torch
+    from helpers import GpuRun
+    s, p = system
+    L = nbk.ResidentLayout(s, p, shuffle_seed=13)
+    order = torch.zeros(len(L.ids), dtype=torch.int32, device="cuda")
+    L.sort_patch_atoms(order)
+    xyzq = torch.zeros((p.atomStorageSize, 4), dtype=torch.float32, device="cuda")
+    L.set_compute_positions(order, xyzq)
+    run = GpuRun(p)
+    run.nb.set_exclusions_by_atom(L.excl_by_atom)
+    run.nb.update_vdw_types_excl_device(L, order)
+    run.nb.build_tile_lists(p, xyzq=xyzq)
+    _, _, _, X = run.eval(ALL | nbk.NBK_PAIRLIST, xyzq=xyzq)
+    n = len(L.ids)
+    rng = np.random.default_rng(5)
+    bond = [rng.normal(size=(3, n)) for _ in range(3)]
+    pmef = rng.normal(size=(n, 3)).astype(np.float32)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    outs = [torch.full((3, n), np.nan, dtype=torch.float64, device="cuda") for _ in range(3)]
+    run.nb.accumulate_forces_to_soa(L, order, 2, *outs, f_bond=dev(bond[0]),
+                                    f_bond_nbond=dev(bond[1]), f_bond_slow=dev(bond[2]),
+                                    f_pme=dev(pmef))
+    normal, nbond, slow = (o.cpu().numpy() for o in outs)
+    o = order.cpu().numpy()
+    slot_of_buf = np.empty(n, dtype=np.int64)
+    for q in range(L.numPatches):
+        b, nb, k = L.records[q, 1], L.records[q, 2], L.records[q, 3]
+        slot_of_buf[b + o[b:b + k]] = nb + np.arange(k)
+    fixed = X.astype(np.int64)[:, slot_of_buf].astype(np.float64) * (1.0 / 4294967296.0)
+    assert np.array_equal(normal, bond[0])
+    assert np.array_equal(nbond, fixed[:3] + bond[1])
+    assert np.array_equal(slow, (pmef.T.astype(np.float64) + fixed[3:]) + bond[2])
+    # level 0 leaves the other arrays untouched
+    keep = [torch.full((3, n), 7.0, dtype=torch.float64, device="cuda") for _ in range(2)]
+    run.nb.accumulate_forces_to_soa(L, order, 0, outs[0], *keep)
+    assert bool((keep[0] == 7.0).all()) and bool((keep[1] == 7.0).all())
