@@ -112,3 +112,42 @@ def test_deterministic(mixed):
     F1 = X1[:3].T.astype(np.float64)[real]
     F2 = X2[:3].T.astype(np.float64)[real]
     assert rms_rel(F2, F1) <= FORCE_RMS_TOL
+
+
+def _sparse_case(s):
+    p = nbk.Packed(s)
+    o = oracle.Oracle(p, PARAMS)
+    keys, nex = o.pairs()
+    run = GpuRun(p)
+    run.build()
+    F, S, res, _ = run.eval(ALL | nbk.NBK_PAIRLIST | nbk.NBK_CORRECTIONS | nbk.NBK_ENERGY_FP64)
+    tl, ja, ex = run.nb.export_tile_lists()
+    mine = nbk.pairs_from_tile_lists(tl, ja, ex, p.atomStorageSize)
+    assert np.array_equal(mine, keys)
+    assert run.nb.stat().numExcluded == nex
+    Fo, So, ro = o.forces(3)
+    real = real_slots(p)
+    scale = max(np.abs(Fo[real]).max(), np.abs(So[real]).max(), 1e-30)
+    assert np.abs(F[real] - Fo[real]).max() <= 1e-5 * scale
+    assert np.abs(S[real] - So[real]).max() <= 1e-5 * scale
+    for k in ("energyVdw", "energyElec", "energySlow"):
+        assert abs(res[k] - ro[k]) <= 1e-6 * max(abs(ro[k]), 1e-12), (k, res[k], ro[k])
+    # the steady step on the same (possibly empty) lists
+    F2, S2, res2, _ = run.eval(ALL | nbk.NBK_CORRECTIONS | nbk.NBK_ENERGY_FP64)
+    assert np.abs(F2[real] - Fo[real]).max() <= 1e-5 * scale
+    return len(keys), int(p.patches[:, 0].astype(bool).sum()), len(p.patches)
+
+
+def test_single_molecule_no_pairs():
+    """One water in a 28 A box: its three pairs are excluded and its images
+    lie beyond the pairlist distance, so every tile list is empty after the
+    refinement and only the excluded-pair corrections act; 6 of the 8 patches
+    are empty."""
+    npairs, full, total = _sparse_case(nbk.System(nbk.NBK_SYS_WATER, 4, 3, 0.0, box=(28.0, 28.0, 28.0)))
+    assert npairs == 0 and full == 2 and total == 8
+
+
+def test_sparse_system_with_empty_patches():
+    """30 waters in a 45 A box: most patches are empty, the lists are ragged."""
+    npairs, full, total = _sparse_case(nbk.System(nbk.NBK_SYS_WATER, 5, 90, 0.0, box=(45.0, 45.0, 45.0)))
+    assert npairs > 0 and full < total
