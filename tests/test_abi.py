@@ -55,3 +55,40 @@ def test_record_layouts_match_reference():
     assert C.sizeof(nbk.VirialEnergy) == 31 * 8
     assert nbk.ComputeRecord.offsetXYZ.offset == 8
     assert nbk.TileList.patchInd.offset == 24 and nbk.TileList.icompute.offset == 40
+
+
+def test_header_compiles_as_c_with_reference_strides(tmp_path):
+    """include/nbk.h is plain C: a C translation unit sees the same record
+    sizes, including the 128-byte CudaLocalRecord of the GPU-resident calls."""
+    import subprocess
+    src = tmp_path / "abi.c"
+    src.write_text(
+        '#include "nbk.h"\n'
+        "_Static_assert(sizeof(nbk_compute_record) == 24, \"compute record\");\n"
+        "_Static_assert(sizeof(nbk_tile_list) == 48, \"tile list\");\n"
+        "_Static_assert(sizeof(nbk_local_record) == 128, \"local record\");\n"
+        "_Static_assert(sizeof(nbk_pme_grid) == 16, \"pme grid\");\n"
+        "_Static_assert(sizeof(nbk_double3) == 24, \"double3\");\n"
+        "int main(void) { return 0; }\n")
+    r = subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        "-c", str(src), "-o", str(tmp_path / "abi.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_pme_and_resident_entry_points_reject_bad_arguments():
+    L = nbk.dev_lib()
+    vp = C.c_void_p
+    assert L.nbk_pme_create(0, None, 0.3, None) == -1
+    g = nbk.PmeGrid(4, 4, 4, 4)                 # grid below the minimum size
+    h = vp()
+    assert L.nbk_pme_create(0, C.byref(g), 0.3, C.byref(h)) == -1
+    g = nbk.PmeGrid(32, 32, 32, 5)              # unsupported order
+    assert L.nbk_pme_create(0, C.byref(g), 0.3, C.byref(h)) == -1
+    assert L.nbk_pme_spread_charge(None, 0, None, None) == -1
+    assert L.nbk_pme_destroy(None) == 0
+    assert L.nbk_sort_patch_atoms(1, None, 64, None, None, None, None, None, None, None) == -1
+    assert L.nbk_set_compute_positions(1, None, None, None, None, 1.0, None, None, None, None,
+                                       None, None) == -1
+    assert L.nbk_update_vdw_types_excl_device(None, 1, 32, None, None, None, None, None, None) == -1
+    assert L.nbk_accumulate_forces_to_soa(None, 2, 1, *([None] * 5), 0, None,
+                                          *([None] * 9), None) == -1
