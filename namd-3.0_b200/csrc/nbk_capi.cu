@@ -106,7 +106,10 @@ struct nbk_context {
   DBuf<nbk_tile_excl> excl1;
   DBuf<int> jtileActive, listActive;
   // compacted lists for steady-state evaluations
-  DBuf<nbk_tile_list> lists2;
+  DBuf<nbk_tile_list> lists2;      // refined, compacted lists, longest first
+  DBuf<nbk_tile_list> listsCompact;  // the compaction's output before the sort
+  DBuf<int> lenHist;                 // list-length histogram / cursors of the sort
+  int maxListLen = 0;                // most j tiles a culled list can hold
   DBuf<int> jatom2;
   DBuf<nbk_tile_excl> excl2;
   DBuf<int> counters;  // [0] lists kept, [1] j tiles kept, [2] force / [3] refine work counters
@@ -393,6 +396,8 @@ NBK_API int nbk_destroy(nbk_handle h) {
   h->jtileActive.release();
   h->listActive.release();
   h->lists2.release();
+  h->listsCompact.release();
+  h->lenHist.release();
   h->jatom2.release();
   h->excl2.release();
   h->counters.release();
@@ -538,6 +543,7 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
                              cudaMemcpyHostToDevice, st), "nbk_build_tile_lists");
     h->hSeeds.clear();
     long long jcap = 0;
+    int maxT2 = 0;
     for (int ci = 0; ci < h->numComputes; ++ci) {
       const nbk_compute_record& cr = h->hComputes[ci];
       if (cr.patchInd.x < 0 || cr.patchInd.x >= numPatches || cr.patchInd.y < 0 ||
@@ -545,6 +551,7 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
         return setErr(NBK_ERR_ARG, "nbk_build_tile_lists: compute refers to a missing patch");
       const int t1 = (hp[cr.patchInd.x].numAtoms + 31) / 32;
       const int t2 = (hp[cr.patchInd.y].numAtoms + 31) / 32;
+      maxT2 = std::max(maxT2, t2);
       for (int it = 0; it < t1; ++it) {
         h->hSeeds.push_back(ListSeed{ci, it, (int)jcap, 0});
         jcap += t2;
@@ -554,6 +561,7 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
       return setErr(NBK_ERR_OVERFLOW, "nbk_build_tile_lists: j-tile capacity exceeds 2^30");
     h->numLists = (int)h->hSeeds.size();
     h->jcap = (int)jcap;
+    h->maxListLen = maxT2;
     NBK_CUDA(h->seeds.ensure(std::max(h->numLists, 1)), "nbk_build_tile_lists");
     if (h->numLists)
       NBK_CUDA(cudaMemcpyAsync(h->seeds.p, h->hSeeds.data(), sizeof(ListSeed) * h->numLists,
@@ -654,13 +662,17 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     NBK_CUDA(launchRefine(r, h->numSM, st), "pairlist refinement");
     const int nl = std::max(h->numLists, 1), nj = std::max(h->jcap, 1);
     NBK_CUDA(h->lists2.ensure(nl), "nbk_nonbonded_force");
+    NBK_CUDA(h->listsCompact.ensure(nl), "nbk_nonbonded_force");
+    NBK_CUDA(h->lenHist.ensure((size_t)h->maxListLen + 1), "nbk_nonbonded_force");
     NBK_CUDA(h->jatom2.ensure(nj), "nbk_nonbonded_force");
     NBK_CUDA(h->excl2.ensure(nj), "nbk_nonbonded_force");
     NBK_CUDA(cudaMemsetAsync(h->counters.p, 0, sizeof(int) * 2, st), "nbk_nonbonded_force");
     NBK_CUDA(launchCompact(h->numLists, h->lists1.p, h->listActive.p, h->jtileActive.p, h->jatom1.p,
-                           h->excl1.p, h->lists2.p, h->jatom2.p, h->excl2.p, h->counters.p,
+                           h->excl1.p, h->listsCompact.p, h->jatom2.p, h->excl2.p, h->counters.p,
                            h->numSM, st), "tile-list compaction");
-    h->launches += 2;
+    NBK_CUDA(launchSortLists(h->numLists, h->listsCompact.p, h->counters.p, h->maxListLen,
+                             h->lenHist.p, h->lists2.p, h->numSM, st), "tile-list sort");
+    h->launches += 5;
     h->refined = true;
   }
   // compacted lists (the pairlist block above may have grown these buffers)

@@ -16,6 +16,11 @@ cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int n
 // a.tileExcls, a.jtileActive, a.listActive and the excluded-pair counts.
 cudaError_t launchRefine(const ForceArgs& a, int numSM, cudaStream_t st);
 
+// The compacted lists [0, *numListsDev) of src copied to dst in order of
+// decreasing j-tile count (lengths clamped to maxLen); hist: maxLen + 1 ints.
+cudaError_t launchSortLists(int numListsMax, const nbk_tile_list* src, const int* numListsDev,
+                            int maxLen, int* hist, nbk_tile_list* dst, int numSM, cudaStream_t st);
+
 cudaError_t launchBBoxes(int numTiles, const float4* xyzq, BBox* bb, cudaStream_t st);
 
 cudaError_t launchBuildLists(int numLists, const ListSeed* seeds,
