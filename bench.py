@@ -236,6 +236,40 @@ def resident_timing(sys_, packed, local_rank, stream, reps=20):
     return out
 
 
+def tile_build_timing(nb, packed, x, stream, reps=20):
+    """Tile-list build (bounding boxes + bbox culling, nbk_build_tile_lists) on
+    device-resident positions, timed with CUDA events (mean of `reps` builds,
+    all enqueued while the GPU sleeps). Unit: (i-tile, j-tile) box tests; a
+    self compute tests j-tile >= i-tile only. Algorithmic bytes: xyzq read for
+    the boxes (16 B per slot), one box written (24 B per tile), one j box read
+    per test (24 B) and one list record written per (compute, i-tile) (48-B tile
+    list + 16-B patch pair); the 4-B j-tile starts of the survivors are left
+    out, so the figure is a lower bound."""
+    import torch
+    st = stream.cuda_stream
+    tiles = (packed.patches[:, 0] + 31) // 32
+    ci, cj = packed.computes_patch[:, 0], packed.computes_patch[:, 1]
+    t1, t2 = tiles[ci].astype(np.int64), tiles[cj].astype(np.int64)
+    zero = ~np.any(packed.computes_offset != 0, axis=1)
+    self_ = (ci == cj) & zero
+    tests = int(np.where(self_, t1 * (t1 + 1) // 2, t1 * t2).sum())
+    lists = int(t1.sum())
+    n = packed.atomStorageSize
+    alg = 16 * n + 24 * (n // 32) + 24 * tests + 64 * lists
+    nb.build_tile_lists(packed, xyzq=x, stream=st)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda._sleep(50_000_000)
+    a.record(stream)
+    for _ in range(reps):
+        nb.build_tile_lists(packed, xyzq=x, stream=st)
+    b.record(stream)
+    torch.cuda.synchronize(stream.device)
+    us = a.elapsed_time(b) * 1e3 / reps
+    return {"us": us, "tile_pairs_tested": tests, "tile_lists": lists,
+            "tile_pairs_per_s": tests / (us * 1e-6), "alg_bytes": alg,
+            "achieved_gbs": alg / (us * 1e-6) / 1e9}
+
+
 def pme_timing(sys_, local_rank, stream, reps=20):
     """PME reciprocal space for the same atoms (nbk_pme_*): grid ~1 A (FFT-friendly
     sizes), B-spline order 4, the short-range path's Ewald coefficient; each
@@ -445,6 +479,9 @@ def run_gpu(args, rank, world, local_rank):
     e2e = {"value": e2e_pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
            "d2h_bytes_per_step": 2 * 16 * n + 8 * 31, "steps": ke}
 
+    build_t = tile_build_timing(nb, packed, frames[0], stream)
+    nb.force(packed, FL | nbk.NBK_PAIRLIST, xyzq=frames[0], d_forces=dF, d_forcesSlow=dS,
+             stream=st)
     resident = resident_timing(sys_, packed, local_rank, stream)
     pme_t = pme_timing(sys_, local_rank, stream)
 
@@ -466,6 +503,7 @@ def run_gpu(args, rank, world, local_rank):
             "evals_per_s": args.steps / (total_ms * 1e-3) * world,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks,
+            "tile_build": build_t,
             "resident_marshaling": resident,
             "pme_reciprocal": pme_t,
             "wall_s_timed_region": wall,

@@ -108,6 +108,11 @@ struct nbk_context {
   // compacted lists for steady-state evaluations
   DBuf<nbk_tile_list> lists2;      // refined, compacted lists, longest first
   DBuf<nbk_tile_list> listsCompact;  // the compaction's output before the sort
+  // Batched replicas skip the sort: lists in compaction order stay grouped by
+  // replica (per-replica LJ rows and accumulators stay hot), and a launch
+  // over many replicas holds enough lists that its tail is short anyway.
+  bool listsSorted = false;
+  const nbk_tile_list* refinedLists() const { return listsSorted ? lists2.p : listsCompact.p; }
   DBuf<int> lenHist;                 // list-length histogram / cursors of the sort
   int maxListLen = 0;                // most j tiles a culled list can hold
   DBuf<int> jatom2;
@@ -257,7 +262,7 @@ ForceArgs refinedForceArgs(nbk_context* h, float cutoff2) {
     a.repLat = h->repLat.p;
     a.repLJ = h->repLJ.p;
   }
-  a.lists = h->lists2.p;
+  a.lists = h->refinedLists();
   a.numListsDev = h->counters.p;
   a.numListsHost = 0;
   a.tileJatomStart = h->jatom2.p;
@@ -670,13 +675,17 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     NBK_CUDA(launchCompact(h->numLists, h->lists1.p, h->listActive.p, h->jtileActive.p, h->jatom1.p,
                            h->excl1.p, h->listsCompact.p, h->jatom2.p, h->excl2.p, h->counters.p,
                            h->numSM, st), "tile-list compaction");
-    NBK_CUDA(launchSortLists(h->numLists, h->listsCompact.p, h->counters.p, h->maxListLen,
-                             h->lenHist.p, h->lists2.p, h->numSM, st), "tile-list sort");
-    h->launches += 5;
+    h->listsSorted = h->nrep == 0;
+    if (h->listsSorted) {
+      NBK_CUDA(launchSortLists(h->numLists, h->listsCompact.p, h->counters.p, h->maxListLen,
+                               h->lenHist.p, h->lists2.p, h->numSM, st), "tile-list sort");
+      h->launches += 3;
+    }
+    h->launches += 2;
     h->refined = true;
   }
   // compacted lists (the pairlist block above may have grown these buffers)
-  a.lists = h->lists2.p;
+  a.lists = h->refinedLists();
   a.tileJatomStart = h->jatom2.p;
   a.tileExcls = h->excl2.p;
   NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
@@ -797,7 +806,7 @@ NBK_API int nbk_export_tile_lists(nbk_handle h, int* numTileLists, int* numJtile
   *numTileLists = cnt[0];
   *numJtiles = cnt[1];
   if (tl && cnt[0])
-    NBK_CUDA(cudaMemcpy(tl, h->lists2.p, sizeof(nbk_tile_list) * cnt[0], cudaMemcpyDeviceToHost), "export");
+    NBK_CUDA(cudaMemcpy(tl, h->refinedLists(), sizeof(nbk_tile_list) * cnt[0], cudaMemcpyDeviceToHost), "export");
   if (jatom && cnt[1])
     NBK_CUDA(cudaMemcpy(jatom, h->jatom2.p, sizeof(int) * cnt[1], cudaMemcpyDeviceToHost), "export");
   if (excl && cnt[1])
@@ -834,7 +843,7 @@ NBK_API int nbk_adjoint(nbk_handle h, unsigned flags, const nbk_float4* d_wF, co
   NBK_CUDA(cudaMemsetAsync(d_gradAB, 0, sizeof(double) * 2 * (size_t)dim * dim, st), "nbk_adjoint");
   NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_adjoint");
   AdjArgs a{};
-  a.lists = h->lists2.p;
+  a.lists = h->refinedLists();
   a.numListsDev = h->counters.p;
   a.tileJatomStart = h->jatom2.p;
   a.tileExcls = h->excl2.p;
