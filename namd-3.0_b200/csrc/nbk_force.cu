@@ -59,10 +59,11 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     forceKernel(const __grid_constant__ ForceArgs a) {
   extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
   __shared__ float4 s_xyzq[kForceWarps][kWarp];
-  // packed loop: the j tile as five rows (x, y, z, q, type bits), each stored
-  // twice in a row (entries j and j + 32) so that j = (lane + k) & 31 and
-  // j ^ 16 are the fixed offsets lane + k and lane + k + 16 from one address
-  __shared__ float s_jt[kForceWarps][5][2 * kWarp];
+  // packed loop: the j tile as five rows (x, y, z, q, type bits) of 64
+  // entries; entry m holds the values of atoms m & 31 and (m & 31) ^ 16, so
+  // that the two packed elements of iteration k, j = (lane + k) & 31 and
+  // j ^ 16, come from one 8-byte load at the fixed offset lane + k
+  __shared__ float2 s_jt[kForceWarps][5][2 * kWarp];
   __shared__ int s_type[kForceWarps][kWarp];
   // FP32 mode: each lane's i force of the current list part in fixed point,
   // folded in at the end of every j tile, so that the sums do not depend on
@@ -173,11 +174,18 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
       const float4 xj = a.xyzq[jstart + lane];
       if constexpr (!doE64) {
         const float tyj = __int_as_float(a.vdwTypes[jstart + lane]);
-        s_jt[wib][0][lane] = s_jt[wib][0][lane + kWarp] = xj.x;
-        s_jt[wib][1][lane] = s_jt[wib][1][lane + kWarp] = xj.y;
-        s_jt[wib][2][lane] = s_jt[wib][2][lane + kWarp] = xj.z;
-        s_jt[wib][3][lane] = s_jt[wib][3][lane + kWarp] = xj.w;
-        s_jt[wib][4][lane] = s_jt[wib][4][lane + kWarp] = tyj;
+        // entry m holds (atom m & 31, atom (m & 31) ^ 16): one 8-byte load
+        // gives both packed elements of an iteration
+        const float2 ex = make_float2(xj.x, __shfl_xor_sync(0xffffffffu, xj.x, 16));
+        const float2 ey = make_float2(xj.y, __shfl_xor_sync(0xffffffffu, xj.y, 16));
+        const float2 ez = make_float2(xj.z, __shfl_xor_sync(0xffffffffu, xj.z, 16));
+        const float2 eq = make_float2(xj.w, __shfl_xor_sync(0xffffffffu, xj.w, 16));
+        const float2 et = make_float2(tyj, __shfl_xor_sync(0xffffffffu, tyj, 16));
+        s_jt[wib][0][lane] = s_jt[wib][0][lane + kWarp] = ex;
+        s_jt[wib][1][lane] = s_jt[wib][1][lane + kWarp] = ey;
+        s_jt[wib][2][lane] = s_jt[wib][2][lane + kWarp] = ez;
+        s_jt[wib][3][lane] = s_jt[wib][3][lane + kWarp] = eq;
+        s_jt[wib][4][lane] = s_jt[wib][4][lane + kWarp] = et;
       } else {
         s_xyzq[wib][lane] = xj;
       }
@@ -204,21 +212,21 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
         for (int k = 0; k < 16; ++k, mk >>= 1) {
           if (!((stepMask >> k) & 0x10001u)) continue;  // warp-uniform
           // element x: j = (lane + k) & 31, element y: j ^ 16
-          const float* pA = &s_jt[wib][0][lane + k];
-          const float* pB = pA + 16;
-          const float2 X = make_float2(pA[0], pB[0]);
-          const float2 Y = make_float2(pA[64], pB[64]);
-          const float2 Z = make_float2(pA[128], pB[128]);
+          const float2* pA = &s_jt[wib][0][lane + k];
+          const float2 X = pA[0];
+          const float2 Y = pA[64];
+          const float2 Z = pA[128];
           const float2 DX = add2(X, nXi), DY = add2(Y, nYi), DZ = add2(Z, nZi);
           const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
           const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
           const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
           if (!__any_sync(0xffffffffu, aA || aB)) continue;
           if (doEnergy) npair += (int)aA + (int)aB;
-          const int tyA = __float_as_int(pA[256]), tyB = __float_as_int(pB[256]);
+          const float2 TY = pA[256];
+          const int tyA = __float_as_int(TY.x), tyB = __float_as_int(TY.y);
           const float2 abA = doBatch ? __ldg(&ljRow[ti + tyA]) : s_lj[ti + tyA];
           const float2 abB = doBatch ? __ldg(&ljRow[ti + tyB]) : s_lj[ti + tyB];
-          const float2 QQ = mul2(f2(xi.w), make_float2(pA[192], pB[192]));
+          const float2 QQ = mul2(f2(xi.w), pA[192]);
           const float2 r2s = make_float2(aA ? R2.x : c.cutoff2, aB ? R2.y : c.cutoff2);
           const float2 qqs = make_float2(aA ? QQ.x : 0.f, aB ? QQ.y : 0.f);
           const float2 As = make_float2(aA ? abA.x : 0.f, aB ? abB.x : 0.f);
