@@ -194,7 +194,10 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
  * Forces are accumulated deterministically as 64-bit fixed point (2^32 per
  * kcal/mol/A) and then written as float4 to any non-NULL output:
  *   d_forces / d_forcesSlow : device float4[atomStorageSize] (w = 0)
- *   h_forces / h_forcesSlow : host float4[atomStorageSize], copied on `stream`
+ *   h_forces / h_forcesSlow : host float4[atomStorageSize] (needs the matching
+ *                             device buffer); page-locked memory is written by
+ *                             the finalizing kernel itself, other host memory
+ *                             by a copy on `stream` after it
  *   d_forcesFixed           : device int64[6*atomStorageSize] SoA
  *                             (fx, fy, fz, fslowx, fslowy, fslowz)
  * With NBK_PAIRLIST the tile lists are refined: masks of pairs within the
@@ -208,7 +211,8 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
 
 /* CudaComputeNonbondedKernel::reduceVirialEnergy, src/CudaComputeNonbondedKernel.cu:3595-3631.
  * Writes the energies and virials of the last nbk_nonbonded_force into
- * ve (device pointer if veOnDevice, else host pointer copied on `stream`). */
+ * ve (device pointer if veOnDevice, else host pointer: page-locked memory is
+ * written by the read-out kernel, other memory by a copy on `stream`). */
 NBK_API int nbk_reduce_virial_energy(nbk_handle h, unsigned flags, nbk_virial_energy* ve,
                                      int veOnDevice, void* stream);
 

@@ -730,25 +730,27 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     sv.compRep = h->nrep ? h->compRep.p : nullptr;
     sv.repLat = h->nrep ? h->repLat.p : nullptr;
   }
+  if ((h_forces && !d_forces) || (h_forcesSlow && !d_forcesSlow))
+    return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: host force output needs the matching device buffer");
+  // page-locked host outputs are written by the finalize kernel itself;
+  // other host memory gets a copy after it
+  float4* hF = static_cast<float4*>(mappedHostPointer(h_forces));
+  float4* hS = (flags & NBK_SLOW) ? static_cast<float4*>(mappedHostPointer(h_forcesSlow)) : nullptr;
   NBK_CUDA(launchFinalizeForces(n, h->force.p, n, h->xyzq, reinterpret_cast<float4*>(d_forces),
                                 (flags & NBK_SLOW) ? reinterpret_cast<float4*>(d_forcesSlow) : nullptr,
                                 flags, h->acc.p, h->numSM, st, h->nrep ? h->slotRep.p : nullptr,
-                                &sv),
+                                &sv, hF, hS),
            "force finalize");
   if ((flags & NBK_VIRIAL) || d_forces || d_forcesSlow) h->launches += 1;
   if (d_forcesFixed)
     NBK_CUDA(cudaMemcpyAsync(d_forcesFixed, h->force.p, sizeof(long long) * 6 * (size_t)n,
                              cudaMemcpyDeviceToDevice, st), "nbk_nonbonded_force: fixed-point copy");
-  if (h_forces || h_forcesSlow) {
-    if ((h_forces && !d_forces) || (h_forcesSlow && !d_forcesSlow))
-      return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: host force output needs the matching device buffer");
-    if (h_forces)
-      NBK_CUDA(cudaMemcpyAsync(h_forces, d_forces, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, st),
-               "nbk_nonbonded_force: D2H");
-    if (h_forcesSlow && (flags & NBK_SLOW))
-      NBK_CUDA(cudaMemcpyAsync(h_forcesSlow, d_forcesSlow, sizeof(float4) * (size_t)n,
-                               cudaMemcpyDeviceToHost, st), "nbk_nonbonded_force: D2H");
-  }
+  if (h_forces && !hF)
+    NBK_CUDA(cudaMemcpyAsync(h_forces, d_forces, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, st),
+             "nbk_nonbonded_force: D2H");
+  if (h_forcesSlow && (flags & NBK_SLOW) && !hS)
+    NBK_CUDA(cudaMemcpyAsync(h_forcesSlow, d_forcesSlow, sizeof(float4) * (size_t)n,
+                             cudaMemcpyDeviceToHost, st), "nbk_nonbonded_force: D2H");
   h->lastFlags = flags;
   return NBK_OK;
 }
@@ -762,10 +764,12 @@ NBK_API int nbk_reduce_virial_energy(nbk_handle h, unsigned flags, nbk_virial_en
   if (h->nrep > 0)
     return setErr(NBK_ERR_STATE, "nbk_reduce_virial_energy: the handle holds replicas; use nbk_reduce_virial_energy_batch");
   cudaStream_t st = (cudaStream_t)stream;
-  nbk_virial_energy* dst = veOnDevice ? ve : h->ve.p;
+  // page-locked host output: the read-out kernel writes it directly
+  nbk_virial_energy* mapped = veOnDevice ? nullptr : static_cast<nbk_virial_energy*>(mappedHostPointer(ve));
+  nbk_virial_energy* dst = veOnDevice ? ve : (mapped ? mapped : h->ve.p);
   NBK_CUDA(launchEnergyVirial(h->acc.p, dst, st), "energy/virial read-out");
   h->launches += 1;
-  if (!veOnDevice)
+  if (!veOnDevice && !mapped)
     NBK_CUDA(cudaMemcpyAsync(ve, h->ve.p, sizeof(nbk_virial_energy), cudaMemcpyDeviceToHost, st),
              "nbk_reduce_virial_energy: D2H");
   return NBK_OK;

@@ -268,7 +268,8 @@ constexpr int kFinalizeThreads = 256;
 __global__ void __launch_bounds__(kFinalizeThreads)
     finalizeKernel(int n, const long long* __restrict__ F, int stride,
                    const float4* __restrict__ xyzq, float4* __restrict__ outF,
-                   float4* __restrict__ outS, int doSlow, int doVirial,
+                   float4* __restrict__ outS, float4* __restrict__ outFH,
+                   float4* __restrict__ outSH, int doSlow, int doVirial,
                    long long* __restrict__ accBase, const int* __restrict__ slotRep,
                    const ShiftVirialArgs shift) {
   long long v[18] = {};
@@ -301,12 +302,15 @@ __global__ void __launch_bounds__(kFinalizeThreads)
       gy = F[4 * (size_t)stride + i];
       gz = F[5 * (size_t)stride + i];
     }
-    if (outF)
-      outF[i] = make_float4((float)(fx * kForceScaleInv), (float)(fy * kForceScaleInv),
-                            (float)(fz * kForceScaleInv), 0.0f);
-    if (outS)
-      outS[i] = make_float4((float)(gx * kForceScaleInv), (float)(gy * kForceScaleInv),
-                            (float)(gz * kForceScaleInv), 0.0f);
+    const float4 f4 = make_float4((float)(fx * kForceScaleInv), (float)(fy * kForceScaleInv),
+                                  (float)(fz * kForceScaleInv), 0.0f);
+    const float4 g4 = make_float4((float)(gx * kForceScaleInv), (float)(gy * kForceScaleInv),
+                                  (float)(gz * kForceScaleInv), 0.0f);
+    if (outF) outF[i] = f4;
+    if (outS) outS[i] = g4;
+    // page-locked host outputs: the stores cross PCIe while the kernel runs
+    if (outFH) outFH[i] = f4;
+    if (outSH) outSH[i] = g4;
     if (doVirial) {
       const float4 x = xyzq[i];
       const double X[3] = {(double)x.x, (double)x.y, (double)x.z};
@@ -393,41 +397,52 @@ __global__ void __launch_bounds__(kFinalizeThreads)
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
                                  int numSM, cudaStream_t st, const int* slotRep,
-                                 const ShiftVirialArgs* shift) {
+                                 const ShiftVirialArgs* shift, float4* outFHost,
+                                 float4* outSHost) {
   if (n <= 0) return cudaSuccess;
   const bool V = flags & NBK_VIRIAL;
-  if (!V && !outF && !outS) return cudaSuccess;
+  if (!V && !outF && !outS && !outFHost && !outSHost) return cudaSuccess;
   const int threads = kFinalizeThreads;
   // two blocks per SM keep enough loads in flight (one per SM left the
   // kernel latency-bound: 11 -> 9 us at 97k slots)
   const int blocks = min((n + threads - 1) / threads, 2 * numSM);
   // the FP64 energy/virial mode accumulates complete pair virials instead
   const bool atomVirial = V && !((flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64));
-  if (!atomVirial && !outF && !outS) return cudaSuccess;
+  if (!atomVirial && !outF && !outS && !outFHost && !outSHost) return cudaSuccess;
   ShiftVirialArgs sv{};
   if (shift && atomVirial) sv = *shift;
-  finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS,
+  finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS, outFHost,
+                                             outSHost,
                                              (flags & NBK_SLOW) ? 1 : 0, atomVirial ? 1 : 0, acc,
                                              slotRep, sv);
   return cudaGetLastError();
 }
 
+void* mappedHostPointer(void* p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes at{};
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+}
+
 __global__ void energyVirialKernel(const long long* __restrict__ accBase, nbk_virial_energy* outBase) {
   const int t = threadIdx.x;
   const long long* acc = accBase + (size_t)blockIdx.x * kAccCount;
-  nbk_virial_energy* out = outBase + blockIdx.x;
-  double* o = reinterpret_cast<double*>(out);
+  double* o = reinterpret_cast<double*>(outBase + blockIdx.x);
   const int nd = (int)(sizeof(nbk_virial_energy) / sizeof(double));
-  if (t < nd) o[t] = 0.0;
-  __syncwarp();
-  if (t < 9) {
-    out->virial[t] = (double)acc[kAccVir + t] * kEnergyScaleInv;
-    out->virialSlow[t] = (double)acc[kAccVirSlow + t] * kEnergyScaleInv;
-  }
-  if (t == 0) {
-    out->energyVdw = (double)acc[kAccEVdw] * kEnergyScaleInv;
-    out->energyElec = (double)acc[kAccEElec] * kEnergyScaleInv;
-    out->energySlow = (double)acc[kAccESlow] * kEnergyScaleInv;
+  // one store per word: virial[9], virialSlow[9], the three energies, then
+  // the FEP / TI / GBIS words (zero); the record may be page-locked host memory
+  if (t < nd) {
+    long long q = 0;
+    if (t < 9) q = acc[kAccVir + t];
+    else if (t < 18) q = acc[kAccVirSlow + t - 9];
+    else if (t == 18) q = acc[kAccEVdw];
+    else if (t == 19) q = acc[kAccEElec];
+    else if (t == 20) q = acc[kAccESlow];
+    o[t] = (double)q * kEnergyScaleInv;
   }
 }
 

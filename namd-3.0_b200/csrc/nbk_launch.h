@@ -70,7 +70,12 @@ struct ShiftVirialArgs {
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
                                  int numSM, cudaStream_t st, const int* slotRep = nullptr,
-                                 const ShiftVirialArgs* shift = nullptr);
+                                 const ShiftVirialArgs* shift = nullptr,
+                                 float4* outFHost = nullptr, float4* outSHost = nullptr);
+
+// Device-visible address of page-locked host memory (the same pointer under
+// unified addressing), or nullptr for any other pointer.
+void* mappedHostPointer(void* p);
 
 // Converts numReplicas accumulator blocks into numReplicas nbk_virial_energy records.
 cudaError_t launchEnergyVirial(const long long* acc, nbk_virial_energy* out, cudaStream_t st,

@@ -98,7 +98,8 @@ class PackedVariant:
     reads both point at the replacements. Only for test inputs."""
 
     _FIELDS = {"atomIndex": "atomIndex", "exclIndexMaxDiff": "exclIndexMaxDiff",
-               "exclusionBits": "exclusionBits", "patches": "patches"}
+               "exclusionBits": "exclusionBits", "patches": "patches", "xyzq": "xyzq"}
+    _DTYPES = {"exclusionBits": np.uint32, "xyzq": np.float32}
 
     def __init__(self, packed, **arrays):
         self.__dict__.update(packed.__dict__)
@@ -106,7 +107,7 @@ class PackedVariant:
         self._keep = []
         v = nbk.PackedView.from_buffer_copy(packed.v)
         for name, arr in arrays.items():
-            arr = np.ascontiguousarray(arr, dtype=np.uint32 if name == "exclusionBits" else np.int32)
+            arr = np.ascontiguousarray(arr, dtype=self._DTYPES.get(name, np.int32))
             self._keep.append(arr)
             setattr(self, name, arr)
             field = self._FIELDS[name]

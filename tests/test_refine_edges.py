@@ -1,6 +1,8 @@
 """Edge cases of the pairlist refinement: exclusion windows wider than the
 kernel's FP32 index test covers (maxdiff above 2896), global atom indices at
-or above 2^24, and fixed atoms (numFreeAtoms < numAtoms).
+or above 2^24, fixed atoms (numFreeAtoms < numAtoms), and pairs placed exactly
+on the pair rule's edges (r^2 equal to plcutoff^2 or cutoff^2 in FP32, and one
+FP32 step inside).
 
 The renumbered and shifted systems carry the same exclusions under new global
 indices, so the oracle's pair set must not change (checked on the CPU, which
@@ -76,6 +78,60 @@ def test_fixed_atoms_change_pairs(base):
     assert np.isin(k2, keys).all()
 
 
+PLCUTOFF, CUTOFF = 13.5, 12.0
+# (x_i, x_j) of the four placed pairs, both atoms in patch 0 with equal y and
+# z: |dx| = 13.5 (r^2 = plcutoff^2: not listed), 13.5 - 2^-20 (listed), 12
+# (r^2 = cutoff^2: listed, not interacting), 12 - 2^-20 (interacting). Every
+# value and difference is exact in FP32.
+EDGE_X = [(-6.75, 6.75), (-6.75 + 2.0 ** -20, 6.75), (-6.0, 6.0), (-6.0 + 2.0 ** -20, 6.0)]
+
+
+def on_edges(system, packed):
+    """Eight water oxygens of patch 0 moved to form the EDGE_X pairs; returns
+    the variant and the slot pairs."""
+    x = packed.xyzq.copy()
+    n, start = int(packed.patches[0, 0]), int(packed.patches[0, 2])
+    slots = np.arange(start, start + n)
+    oxygen = system.lj_table()[0] - 2          # water O type of the mixed systems
+    ox = [int(a) for a in slots if packed.vdwTypes[a] == oxygen][:8]
+    assert len(ox) == 8
+    moved = set(ox)
+    rest = np.array([a for a in slots if a not in moved])
+    grid = [(y, z) for y in np.arange(-6.0, 6.5, 1.5) for z in np.arange(-6.0, 6.5, 1.5)]
+    pairs, used = [], []
+    for m, (xi, xj) in enumerate(EDGE_X):
+        for y, z in grid:
+            if any(abs(y - u) < 2.0 and abs(z - v) < 2.0 for u, v in used):
+                continue
+            cand = np.array([[xi, y, z], [xj, y, z]], np.float32)
+            d = np.linalg.norm(x[rest, None, :3] - cand[None], axis=2).min()
+            if d > 1.2:
+                break
+        else:
+            raise AssertionError("no free place for an edge pair")
+        used.append((y, z))
+        a, b = ox[2 * m], ox[2 * m + 1]
+        x[a, :3], x[b, :3] = cand[0], cand[1]
+        pairs.append((a, b))
+    return PackedVariant(packed, xyzq=x), pairs
+
+
+def _edge_keys(var, pairs):
+    n = np.uint64(var.atomStorageSize)
+    return [np.uint64(min(a, b)) * n + np.uint64(max(a, b)) for a, b in pairs]
+
+
+def test_edge_pairs_fall_on_designed_sides(base):
+    s, p, _ = base
+    var, pairs = on_edges(s, p)
+    r2 = [np.float32(var.xyzq[b, 0] - var.xyzq[a, 0]) ** 2 for a, b in pairs]
+    assert r2[0] == np.float32(PLCUTOFF) ** 2 and r2[1] < np.float32(PLCUTOFF) ** 2
+    assert r2[2] == np.float32(CUTOFF) ** 2 and r2[3] < np.float32(CUTOFF) ** 2
+    keys, _ = oracle.Oracle(var, PARAMS).pairs()
+    listed = np.isin(_edge_keys(var, pairs), unordered_keys(keys, var.atomStorageSize))
+    assert listed.tolist() == [False, True, True, True]
+
+
 def _check(var):
     keys, nex = oracle.Oracle(var, PARAMS).pairs()
     run = GpuRun(var)
@@ -96,12 +152,19 @@ def _check(var):
         assert np.array_equal(rk, unordered_keys(keys, var.atomStorageSize))
         assert rnex == nex
     print(f"pairs {len(keys)} excluded {nex}")
+    return run
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("which", ["interleaved", "shifted", "fixed"])
+@pytest.mark.parametrize("which", ["interleaved", "shifted", "fixed", "edges"])
 def test_refine_edge_pairsets(base, which):
     s, p, _ = base
     var = {"interleaved": lambda: interleaved(s, p), "shifted": lambda: shifted(s, p),
-           "fixed": lambda: with_fixed(p)}[which]()
-    _check(var)
+           "fixed": lambda: with_fixed(p), "edges": lambda: on_edges(s, p)[0]}[which]()
+    run = _check(var)
+    if which == "edges":
+        # interacting pairs (r^2 < cutoff^2 in FP32) counted by the force
+        # kernel equal the oracle's count on the same positions
+        run.eval(ALL)
+        _, _, ro = oracle.Oracle(var, PARAMS).forces(1)
+        assert run.nb.pair_count() == int(ro["pairs"])
