@@ -168,6 +168,8 @@ struct SolveArgs {
   const float* bm3;
   float2* data;         // (K3, K2, nh), x fastest
   double* partial;      // [blocks][7]: energy, virial xx xy xz yy yz zz
+  double* ev;           // energy, virial[9] (row-major)
+  int* done;            // blocks finished (the last one sums the partials, resets it)
   int doEV;
 };
 
@@ -232,29 +234,36 @@ __global__ void __launch_bounds__(kSolveThreads) solveKernel(const __grid_consta
     for (int w = 0; w < kSolveThreads / 32; ++w) s += s_p[w][threadIdx.x];
     a.partial[blockIdx.x * 7 + threadIdx.x] = s;
   }
-}
-
-// Sums the block partials (warp q sums quantity q: lane l the blocks l, l + 32,
-// ..., then a fixed warp tree): energy = 0.5 sum, virial = -0.5 sum
-// (scalar_sum_kernel's final scaling), into ev[0] and ev[1..9] (row-major).
-__global__ void solveFinishKernel(int blocks, const double* __restrict__ partial,
-                                  double* __restrict__ ev) {
-  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (q >= 7) return;  // warp-uniform
-  double s = 0;
-  for (int b = lane; b < blocks; b += 32) s += partial[b * 7 + q];
+  // the last block to finish sums the partials of all blocks in a fixed order
+  // (warp q sums quantity q: lane l the blocks l, l + 32, ..., then a fixed
+  // warp tree): energy = 0.5 sum, virial = -0.5 sum (scalar_sum_kernel's
+  // final scaling), into ev[0] and ev[1..9]
+  __shared__ int s_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(a.done, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int q = wib;
+  if (q < 7) {
+    double s = 0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) s += __ldcg(&a.partial[b * 7 + q]);
 #pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane != 0) return;
-  if (q == 0) {
-    ev[0] = 0.5 * s;
-  } else {
-    // xx xy xz yy yz zz -> row-major 3x3
-    const int map[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
-    const int r = map[q - 1][0], c = map[q - 1][1];
-    ev[1 + 3 * r + c] = -0.5 * s;
-    ev[1 + 3 * c + r] = -0.5 * s;
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      if (q == 0) {
+        a.ev[0] = 0.5 * s;
+      } else {
+        // xx xy xz yy yz zz -> row-major 3x3
+        const int map[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+        const int r = map[q - 1][0], c = map[q - 1][1];
+        a.ev[1 + 3 * r + c] = -0.5 * s;
+        a.ev[1 + 3 * c + r] = -0.5 * s;
+      }
+    }
   }
+  if (threadIdx.x == 0) *a.done = 0;  // ready for the next solve
 }
 
 struct GatherArgs {
@@ -365,6 +374,7 @@ struct nbk_pme_s {
   float* bm = nullptr;                      // bm1 | bm2 | bm3
   double* partial = nullptr;                // solve partials, self-energy partials
   double* ev = nullptr;                     // energy, virial[9]
+  int* done = nullptr;                      // solve blocks finished
   int solveBlocks = 0;
   cufftHandle fwd = 0, bwd = 0;
   bool plans = false;
@@ -444,6 +454,8 @@ extern "C" NBK_API int nbk_pme_create(int deviceID, const nbk_pme_grid* g, doubl
   if (e == cudaSuccess)
     e = cudaMalloc(&p->partial, sizeof(double) * std::max<size_t>(7 * (size_t)p->solveBlocks, 1024));
   if (e == cudaSuccess) e = cudaMalloc(&p->ev, sizeof(double) * 10);
+  if (e == cudaSuccess) e = cudaMalloc(&p->done, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(p->done, 0, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(p->gridFixed, 0, n * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemset(p->ev, 0, sizeof(double) * 10);
   if (e == cudaSuccess) {
@@ -484,6 +496,7 @@ extern "C" NBK_API int nbk_pme_destroy(nbk_pme p) {
   cudaFree(p->bm);
   cudaFree(p->partial);
   cudaFree(p->ev);
+  cudaFree(p->done);
   delete p;
   return NBK_OK;
 }
@@ -547,6 +560,8 @@ extern "C" NBK_API int nbk_pme_solve(nbk_pme p, const double* lattice, unsigned 
   a.bm3 = p->bm + p->K1 + p->K2;
   a.data = p->gridHat;
   a.partial = p->partial;
+  a.ev = p->ev;
+  a.done = p->done;
   a.doEV = (flags & (NBK_ENERGY | NBK_VIRIAL)) ? 1 : 0;
   PME_FFT(cufftSetStream(p->fwd, st), "nbk_pme_solve");
   PME_FFT(cufftSetStream(p->bwd, st), "nbk_pme_solve");
@@ -554,10 +569,6 @@ extern "C" NBK_API int nbk_pme_solve(nbk_pme p, const double* lattice, unsigned 
           "nbk_pme_solve: forward FFT");
   solveKernel<<<p->solveBlocks, kSolveThreads, 0, st>>>(a);
   PME_CUDA(cudaGetLastError(), "nbk_pme_solve");
-  if (a.doEV) {
-    solveFinishKernel<<<1, 7 * 32, 0, st>>>(p->solveBlocks, p->partial, p->ev);
-    PME_CUDA(cudaGetLastError(), "nbk_pme_solve");
-  }
   PME_FFT(cufftExecC2R(p->bwd, reinterpret_cast<cufftComplex*>(p->gridHat), p->gridReal),
           "nbk_pme_solve: backward FFT");
   return NBK_OK;

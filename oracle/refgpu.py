@@ -2,7 +2,9 @@
 tile-list and nonbonded kernels (src/CudaTileListKernel.cu,
 src/CudaComputeNonbondedKernel.cu) built from the reference tree by
 oracle/ref_gpu/Makefile, driven in the order CudaComputeNonbonded::launchWork
-uses (src/CudaComputeNonbonded.C:1440-1530).
+uses (src/CudaComputeNonbonded.C:1440-1530), and its PME kernels
+(src/CudaPmeSolverUtilKernel.cu) driven as CudaPmeOneDevice does
+(src/CudaPmeSolverUtil.C:1364-1650).
 
 Test infrastructure: the tests use it to pin the product's tile-list pair sets
 and forces against the reference kernels themselves and to time the
@@ -41,6 +43,11 @@ def lib() -> C.CDLL:
         L.refgpu_tile_list_sizes.argtypes = [vp, C.POINTER(C.c_int)]
         L.refgpu_tile_lists.argtypes = [vp, vp, vp, vp]
         L.refgpu_destroy.argtypes = [vp]
+        L.refpme_last_error.restype = C.c_char_p
+        L.refpme_create.argtypes = [ip, ip, ip, ip, C.c_double, fp, fp, fp, C.POINTER(vp)]
+        L.refpme_compute.argtypes = [vp, vp, ip, dp, C.c_double, ip, vp, vp]
+        L.refpme_energy_virial.argtypes = [vp, dp]
+        L.refpme_destroy.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -126,3 +133,47 @@ class RefGpu:
         _check(lib().refgpu_tile_lists(self._h, tl.ctypes.data, ja.ctypes.data, ex.ctypes.data),
                "refgpu_tile_lists")
         return tl[:nl], ja[:nj], ex[:nj], nexcl
+
+
+def _pcheck(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what}: {lib().refpme_last_error().decode()}")
+
+
+class RefPme:
+    """The reference's single-device PME kernels on one grid: K (K1, K2, K3),
+    B-spline order, Ewald coefficient and the B-spline moduli per dimension
+    (the values of the reference's compute_b_moduli, passed in FP32 as it
+    does)."""
+
+    def __init__(self, K, order, kappa, moduli):
+        bm = [np.ascontiguousarray(m, np.float32) for m in moduli]
+        self._keep = bm
+        h = C.c_void_p()
+        fpp = C.POINTER(C.c_float)
+        _pcheck(lib().refpme_create(int(K[0]), int(K[1]), int(K[2]), int(order), float(kappa),
+                                    bm[0].ctypes.data_as(fpp), bm[1].ctypes.data_as(fpp),
+                                    bm[2].ctypes.data_as(fpp), C.byref(h)), "refpme_create")
+        self._h = h
+
+    def __del__(self):
+        _l = _lib
+        if getattr(self, "_h", None) and _l is not None:
+            _l.refpme_destroy(self._h)
+            self._h = None
+
+    def compute(self, atoms_ptr, n, lattice, forces_ptr, energy_virial=True, stream=None):
+        """atoms_ptr: device float4[n] fractional atoms; lattice: 3x3 rows a,
+        b, c; forces_ptr: device float3[n] (fractional-gradient forces)."""
+        L = np.asarray(lattice, np.float64).reshape(3, 3)
+        recip = np.ascontiguousarray(np.linalg.inv(L).T)      # rows a*, b*, c*
+        vol = abs(float(np.linalg.det(L)))
+        _pcheck(lib().refpme_compute(self._h, atoms_ptr, int(n),
+                                     recip.reshape(-1).ctypes.data_as(C.POINTER(C.c_double)), vol,
+                                     int(energy_virial), forces_ptr, stream), "refpme_compute")
+
+    def energy_virial(self):
+        out = np.zeros(7, np.float64)
+        _pcheck(lib().refpme_energy_virial(self._h, out.ctypes.data_as(C.POINTER(C.c_double))),
+                "refpme_energy_virial")
+        return out

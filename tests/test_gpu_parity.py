@@ -151,3 +151,37 @@ def test_sparse_system_with_empty_patches():
     """30 waters in a 45 A box: most patches are empty, the lists are ragged."""
     npairs, full, total = _sparse_case(nbk.System(nbk.NBK_SYS_WATER, 5, 90, 0.0, box=(45.0, 45.0, 45.0)))
     assert npairs > 0 and full < total
+
+
+def test_host_outputs_equal_device_outputs(water):
+    """Host force and energy outputs hold exactly the device outputs, both for
+    page-locked memory (written by the kernels over PCIe) and for pageable
+    memory (copied after them)."""
+    import torch
+    s, p, _ = water
+    n = p.atomStorageSize
+    run = GpuRun(p)
+    run.build()
+    run.eval(ALL | nbk.NBK_PAIRLIST)
+    nb = run.nb
+    dF = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    dS = torch.zeros_like(dF)
+    pinF = torch.full((n, 4), 7.0).pin_memory()
+    pinS = torch.full((n, 4), 7.0).pin_memory()
+    pageF = np.full((n, 4), 7.0, np.float32)
+    pageS = np.full((n, 4), 7.0, np.float32)
+    dVE = torch.zeros(31, dtype=torch.float64, device="cuda")
+    pinVE = torch.full((31,), 7.0, dtype=torch.float64).pin_memory()
+    pageVE = np.full(31, 7.0)
+    for hF, hS in ((pinF, pinS), (pageF, pageS)):
+        nb.force(p, ALL, xyzq=p.xyzq, d_forces=dF, d_forcesSlow=dS, h_forces=hF, h_forcesSlow=hS)
+    nb.virial_energy_to(dVE.data_ptr(), True)
+    nb.virial_energy_to(pinVE.data_ptr(), False)
+    nb.virial_energy_to(pageVE.ctypes.data, False)
+    torch.cuda.synchronize()
+    for out, dev in ((pinF.numpy(), dF), (pinS.numpy(), dS), (pageF, dF), (pageS, dS)):
+        assert np.array_equal(out, dev.cpu().numpy())
+    assert np.abs(dF.cpu().numpy()).max() > 0
+    ve = dVE.cpu().numpy()
+    assert np.array_equal(pinVE.numpy(), ve) and np.array_equal(pageVE, ve)
+    assert ve[18] != 0.0 and not ve[21:].any()

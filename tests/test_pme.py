@@ -181,3 +181,81 @@ def test_gpu_ewald_total_is_split_independent():
         scale = max(scale, abs(eself))
     # the total is a small difference of terms of the self energy's size
     assert abs(totals[0] - totals[1]) <= 1e-7 * scale
+
+
+def _ref_case(atoms, L, K, order, d_atoms):
+    import torch
+    import refgpu
+    moduli = [opme.b_moduli(k, order) for k in K]
+    r = refgpu.RefPme(K, order, BETA, moduli)
+    f = torch.zeros((len(atoms), 3), dtype=torch.float32, device="cuda")
+    r.compute(d_atoms.data_ptr(), len(atoms), L, f.data_ptr())
+    ev = r.energy_virial()
+    R = np.linalg.inv(np.asarray(L, np.float64)).T            # rows a*, b*, c*
+    F = f.cpu().numpy().astype(np.float64) @ R                # Lattice::scale_force
+    xx, xy, xz, yy, yz, zz = ev[1:]
+    W = np.array([[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]])
+    return r, F, ev[0], W
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which,order", [("water9k", 4), ("mixed20k", 4), ("mixed20k", 6),
+                                         ("mixed20k", 8), ("triclinic20k", 4)])
+def test_gpu_pme_vs_reference_kernels(which, order):
+    """The reference's own PME kernels (spread_charge_v2, scalar_sum,
+    gather_force with cuFFT, as CudaPmeOneDevice drives them) on the same FP32
+    atoms agree with the product and with the FP64 restatement."""
+    import refgpu
+    if not refgpu.available():
+        pytest.skip("reference kernels not built")
+    atoms, L, K = _systems()[which]
+    _, d_atoms, F, E, W = _gpu_case(atoms, L, K, order)
+    _, Fr, Er, Wr = _ref_case(atoms, L, K, order, d_atoms)
+    Eo, Wo, Fo = opme.pme(atoms, L, K, order, BETA)
+    for tag, (e, f, w) in {"reference": (Er, Fr, Wr), "product": (E, F, W)}.items():
+        ef, fr = abs(e - Eo) / abs(Eo), rms_rel(f, Fo)
+        vr = np.abs(w - Wo).max() / np.abs(Wo).max()
+        print(f"{which} order {order} {tag} vs oracle: energy {ef:.2e} force {fr:.2e} virial {vr:.2e}")
+        assert ef <= PME_ENERGY_TOL and fr <= PME_FORCE_RMS_TOL and vr <= PME_VIRIAL_TOL
+    assert abs(E - Er) <= 2 * PME_ENERGY_TOL * abs(Eo)
+    assert rms_rel(F, Fr) <= 2 * PME_FORCE_RMS_TOL
+
+
+@pytest.mark.gpu
+def test_gpu_pme_reference_timing():
+    """One reciprocal-space evaluation (spread, FFTs, solve with energy and
+    virial, gather) of the 92,224-atom mixed system on a 108x108x80 grid,
+    order 4: the reference's kernels against the product's, CUDA events on one
+    stream with every launch queued while the GPU sleeps."""
+    import torch
+    import refgpu
+    if not refgpu.available():
+        pytest.skip("reference kernels not built")
+    m = nbk.System(nbk.NBK_SYS_MIXED, 2, 92224, 0.3, box=(108.0, 108.0, 78.0))
+    b = m.arrays()
+    L = np.diag(np.asarray(b["box"], dtype=np.float64))
+    atoms = opme.fractional_atoms(np.asarray(b["pos"]).reshape(-1, 3), b["charge"], L,
+                                  qscale=QSCALE)
+    K, order, n = (108, 108, 80), 4, len(atoms)
+    d_atoms = torch.from_numpy(np.ascontiguousarray(atoms)).cuda()
+    f = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    p = nbk.Pme(K, order, BETA)
+    r = refgpu.RefPme(K, order, BETA, [opme.b_moduli(k, order) for k in K])
+    st = torch.cuda.current_stream()
+    calls = {"product": lambda: p.compute(d_atoms, n, L, f, stream=st.cuda_stream),
+             "reference": lambda: r.compute(d_atoms.data_ptr(), n, L, f.data_ptr(),
+                                            stream=st.cuda_stream)}
+    out = {}
+    for name, fn in calls.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda._sleep(50_000_000)
+        a.record(st)
+        for _ in range(20):
+            fn()
+        z.record(st)
+        torch.cuda.synchronize()
+        out[f"{name}_us"] = round(a.elapsed_time(z) * 1e3 / 20, 2)
+    print("pme timing", out)
