@@ -33,7 +33,7 @@
 namespace nbk {
 namespace {
 
-constexpr double kGridScale = 4294967296.0;  // 2^32 fixed-point units per charge unit
+constexpr float kGridScale = 4294967296.0f;  // 2^32 fixed-point units per charge unit
 constexpr int kSolveThreads = 256;
 constexpr int kMaxOrder = 8;
 
@@ -140,7 +140,9 @@ __global__ void __launch_bounds__(128) spreadKernel(int n, const float4* __restr
         if (y >= K2) y -= K2;
         if (z >= K3) z -= K3;
         const float v = s_th[wib][0][x0][m] * s_th[wib][1][y0][m] * s_th[wib][2][z0][m];
-        const long long q = __double2ll_rn((double)v * kGridScale);
+        // v 2^32 is exact in FP32 (a power-of-two scaling), so this is the
+        // same integer as the FP64 product rounded to the nearest
+        const long long q = __float2ll_rn(v * kGridScale);
         atomicAdd(&grid[x + (size_t)K1 * (y + (size_t)K2 * z)], (unsigned long long)q);
       }
     }
@@ -153,7 +155,8 @@ __global__ void gridToFloatKernel(size_t n, unsigned long long* __restrict__ g,
                                   float* __restrict__ out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x) {
-    out[i] = (float)((double)(long long)g[i] * (1.0 / kGridScale));
+    // rounding the integer to FP32, then the exact scaling by 2^-32
+    out[i] = __ll2float_rn((long long)g[i]) * (1.0f / kGridScale);
     g[i] = 0ull;
   }
 }
@@ -289,11 +292,11 @@ __global__ void gatherKernel(const __grid_constant__ GatherArgs a) {
     bsplineThetaD<order>(wy, ty, dy);
     bsplineThetaD<order>(wz, tz, dz);
     float f1 = 0.f, f2 = 0.f, f3 = 0.f;
-#pragma unroll 1
+#pragma unroll 2
     for (int z0 = 0; z0 < order; ++z0) {
       int z = iz + z0;
       if (z >= a.K3) z -= a.K3;
-#pragma unroll 2
+#pragma unroll
       for (int y0 = 0; y0 < order; ++y0) {
         int y = iy + y0;
         if (y >= a.K2) y -= a.K2;
