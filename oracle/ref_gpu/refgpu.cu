@@ -74,8 +74,14 @@ void clear_device_array_async_T(void* data, const size_t ndata, cudaStream_t str
                                 const size_t sizeofT) {
   if (ndata) ck(cudaMemsetAsync(data, 0, ndata * sizeofT, stream), "clear_device_array_async_T");
 }
+// The synchronous clear and the zeroing of new buffers below run on the legacy
+// default stream, which does not order itself with the harness's non-blocking
+// stream: each waits for its memset, so no kernel queued afterwards can run
+// before it (a kernel that did would have its output zeroed after the fact).
 void clear_device_array_T(void* data, const size_t ndata, const size_t sizeofT) {
-  if (ndata) ck(cudaMemset(data, 0, ndata * sizeofT), "clear_device_array_T");
+  if (!ndata) return;
+  ck(cudaMemset(data, 0, ndata * sizeofT), "clear_device_array_T");
+  ck(cudaDeviceSynchronize(), "clear_device_array_T sync");
 }
 void allocate_host_T(void** pp, const size_t len, const size_t sizeofT) {
   ck(cudaMallocHost(pp, len * sizeofT), "allocate_host_T");
@@ -84,6 +90,7 @@ void allocate_host_T(void** pp, const size_t len, const size_t sizeofT) {
 void allocate_device_T(void** pp, const size_t len, const size_t sizeofT) {
   ck(cudaMalloc(pp, len * sizeofT), "allocate_device_T");
   ck(cudaMemset(*pp, 0, len * sizeofT), "allocate_device_T memset");
+  ck(cudaDeviceSynchronize(), "allocate_device_T sync");
 }
 void deallocate_device_T(void** pp) {
   if (*pp) ck(cudaFree(*pp), "deallocate_device_T");
@@ -105,6 +112,7 @@ bool reallocate_device_T(void** pp, size_t* curlen, const size_t newlen, const f
   if (n == 0) n = 1;
   ck(cudaMalloc(pp, n * sizeofT), "reallocate_device_T");
   ck(cudaMemset(*pp, 0, n * sizeofT), "reallocate_device_T memset");
+  ck(cudaDeviceSynchronize(), "reallocate_device_T sync");
   *curlen = n;
   return true;
 }

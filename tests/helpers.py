@@ -173,20 +173,10 @@ def unordered_keys(keys, storage):
     return np.sort(np.minimum(i, j) * n + np.maximum(i, j))
 
 
-def reference_pairs(ref, xyzq, storage, attempts=2):
+def reference_pairs(ref, xyzq, storage):
     """A pairlist evaluation through the reference kernels (a refgpu.RefGpu
-    after setup) and the unordered pairs of their refined tile lists, with the
-    reference's excluded-pair count and the number of re-runs.
-
-    On the B200 the reference's refined lists once came back holding one pair
-    many times (the interleaved-renumbering case; the product's lists, built
-    in the same process, were exact, and three re-runs of the test were
-    clean). An export that lists a pair twice is therefore evaluated again, at
-    most `attempts` times in all; the caller's assertions judge the last one."""
-    for k in range(attempts):
-        ref.eval(1, 1, 1, 1, xyzq)
-        tl, ja, ex, nexcl = ref.tile_lists()
-        keys = unordered_keys(nbk.pairs_from_tile_lists(tl, ja, ex, storage), storage)
-        if len(keys) < 2 or np.all(keys[1:] != keys[:-1]):
-            return keys, nexcl, k
-    return keys, nexcl, attempts - 1
+    after setup): the unordered pairs of their refined tile lists and the
+    reference's excluded-pair count."""
+    ref.eval(1, 1, 1, 1, xyzq)
+    tl, ja, ex, nexcl = ref.tile_lists()
+    return unordered_keys(nbk.pairs_from_tile_lists(tl, ja, ex, storage), storage), nexcl
