@@ -185,3 +185,61 @@ def test_host_outputs_equal_device_outputs(water):
     ve = dVE.cpu().numpy()
     assert np.array_equal(pinVE.numpy(), ve) and np.array_equal(pageVE, ve)
     assert ve[18] != 0.0 and not ve[21:].any()
+
+
+def test_pairlist_and_steady_steps_replay_from_a_cuda_graph(mixed):
+    """With the patch layout unchanged, a whole pairlist step (tile-list build,
+    refinement, compaction, sort, forces, energy read-out) and a steady step
+    are captured in CUDA graphs (no host synchronisation, no allocation) and
+    their replays on new positions give exactly the direct calls' results."""
+    import torch
+    s, p, _ = mixed
+    n = p.atomStorageSize
+    nb = nbk.Nonbonded(PARAMS, s.lj_table())
+    nb.setup(p)
+    x = torch.from_numpy(p.xyzq.copy()).cuda()
+    dF = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    dS = torch.zeros_like(dF)
+    dVE = torch.zeros(31, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+
+    def pairlist_step(cs):
+        nb.build_tile_lists(p, xyzq=x, stream=cs)
+        nb.force(p, ALL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=cs)
+        nb.virial_energy_to(dVE.data_ptr(), True, stream=cs)
+
+    def steady_step(cs):
+        nb.force(p, ALL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=cs)
+        nb.virial_energy_to(dVE.data_ptr(), True, stream=cs)
+
+    with torch.cuda.stream(st):
+        pairlist_step(st.cuda_stream)
+        steady_step(st.cuda_stream)
+    st.synchronize()
+    graphs = []
+    for step in (pairlist_step, steady_step):
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=st):
+            step(torch.cuda.current_stream().cuda_stream)
+        graphs.append(g)
+    rng = np.random.default_rng(11)
+    x0 = x.clone()
+    for k in range(2):
+        moved = x0.clone()
+        moved[:, :3] += torch.from_numpy(rng.normal(0.0, 0.02, (n, 3)).astype(np.float32)).cuda()
+        out = []
+        for use_graph in (True, False):
+            x.copy_(moved)
+            torch.cuda.synchronize()
+            with torch.cuda.stream(st):
+                for g, step in zip(graphs, (pairlist_step, steady_step)):
+                    if use_graph:
+                        g.replay()
+                    else:
+                        step(st.cuda_stream)
+            st.synchronize()
+            out.append((dF.clone(), dS.clone(), dVE.clone()))
+        for a, b in zip(out[0], out[1]):
+            assert torch.equal(a, b)
+        assert out[0][2][18].item() != 0.0
+    del graphs
