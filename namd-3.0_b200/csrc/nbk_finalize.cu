@@ -421,11 +421,14 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
 void* mappedHostPointer(void* p) {
   if (!p) return nullptr;
   cudaPointerAttributes at{};
-  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+  int dev = -1;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess || cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
-  return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+  // page-locked memory of the current device's context only (memory pinned
+  // in another context without the portable flag gets the copy instead)
+  return (at.type == cudaMemoryTypeHost && at.device == dev) ? at.devicePointer : nullptr;
 }
 
 __global__ void energyVirialKernel(const long long* __restrict__ accBase, nbk_virial_energy* outBase) {

@@ -73,8 +73,9 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
                                  const ShiftVirialArgs* shift = nullptr,
                                  float4* outFHost = nullptr, float4* outSHost = nullptr);
 
-// Device-visible address of page-locked host memory (the same pointer under
-// unified addressing), or nullptr for any other pointer.
+// Device-visible address of host memory page-locked in the current device's
+// context (the same pointer under unified addressing), or nullptr for any
+// other pointer.
 void* mappedHostPointer(void* p);
 
 // Converts numReplicas accumulator blocks into numReplicas nbk_virial_energy records.
