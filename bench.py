@@ -137,6 +137,20 @@ def combine_ranks(total_ms: float, pairs: int, dist=None, device=None):
 
 
 # ---------------------------------------------------------------------------
+def host_cpu():
+    """Model name and logical CPU count of the host running the CPU leg."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "logical_cpus": os.cpu_count()}
+
+
 def cpu_eval_sample(packed, budget_s: float, max_evals: int = 1000):
     """Times the CPU restatement (oracle/, all host threads) on whole evaluations
     of the workload until `budget_s` is spent. Returns (pairs/s, threads, sample)."""
@@ -191,6 +205,7 @@ def run_reference(args, rank, world):
         "config": {"workload": WORKLOAD, "parallelism": "host threads"},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "host": host_cpu(),
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
@@ -488,7 +503,8 @@ def run_gpu(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_eval_sample(packed, args.cpu_seconds)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+               "host": host_cpu()}
 
     if rank == 0:
         out = {
