@@ -237,25 +237,29 @@ def test_gpu_pme_reference_timing():
     atoms = opme.fractional_atoms(np.asarray(b["pos"]).reshape(-1, 3), b["charge"], L,
                                   qscale=QSCALE)
     K, order, n = (108, 108, 80), 4, len(atoms)
-    d_atoms = torch.from_numpy(np.ascontiguousarray(atoms)).cuda()
+    # the generation order of the system, and the patch order in which NAMD's
+    # PME receives atoms (patch by patch, each patch in its bisection order)
+    patch_order = np.argsort(nbk.Packed(m).slotOfAtom, kind="stable")
     f = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
     p = nbk.Pme(K, order, BETA)
     r = refgpu.RefPme(K, order, BETA, [opme.b_moduli(k, order) for k in K])
     st = torch.cuda.current_stream()
-    calls = {"product": lambda: p.compute(d_atoms, n, L, f, stream=st.cuda_stream),
-             "reference": lambda: r.compute(d_atoms.data_ptr(), n, L, f.data_ptr(),
-                                            stream=st.cuda_stream)}
     out = {}
-    for name, fn in calls.items():
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize()
-        a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda._sleep(50_000_000)
-        a.record(st)
-        for _ in range(20):
-            fn()
-        z.record(st)
-        torch.cuda.synchronize()
-        out[f"{name}_us"] = round(a.elapsed_time(z) * 1e3 / 20, 2)
+    for tag, idx in (("generation", np.arange(n)), ("patch", patch_order)):
+        d_atoms = torch.from_numpy(np.ascontiguousarray(atoms[idx])).cuda()
+        calls = {"product": lambda: p.compute(d_atoms, n, L, f, stream=st.cuda_stream),
+                 "reference": lambda: r.compute(d_atoms.data_ptr(), n, L, f.data_ptr(),
+                                                stream=st.cuda_stream)}
+        for name, fn in calls.items():
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda._sleep(50_000_000)
+            a.record(st)
+            for _ in range(20):
+                fn()
+            z.record(st)
+            torch.cuda.synchronize()
+            out[f"{tag}_order_{name}_us"] = round(a.elapsed_time(z) * 1e3 / 20, 2)
     print("pme timing", out)
