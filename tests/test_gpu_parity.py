@@ -243,3 +243,20 @@ def test_pairlist_and_steady_steps_replay_from_a_cuda_graph(mixed):
             assert torch.equal(a, b)
         assert out[0][2][18].item() != 0.0
     del graphs
+
+
+def test_refined_lists_are_sorted_longest_first(mixed):
+    """After a pairlist step the compacted tile lists come longest first, and
+    their j-tile ranges still partition the compacted j tiles exactly once."""
+    s, p, _ = mixed
+    run = GpuRun(p)
+    run.build()
+    run.eval(ALL | nbk.NBK_PAIRLIST)
+    tl, ja, _ = run.nb.export_tile_lists()
+    lens = tl[:, 2] - tl[:, 1] + 1          # jtileEnd - jtileStart + 1
+    assert len(lens) > 0 and (lens >= 1).all()
+    assert (np.diff(lens) <= 0).all()
+    order = np.argsort(tl[:, 1])
+    starts, ends = tl[order, 1], tl[order, 2]
+    assert starts[0] == 0 and ends[-1] == len(ja) - 1
+    assert (starts[1:] == ends[:-1] + 1).all()
