@@ -49,10 +49,9 @@ extern "C" {
 #define NBK_CORRECTIONS 16u /* also apply excluded / modified (1-4) pair corrections
                               (reference: ComputeBondedCUDAKernel exclusionForce /
                               modifiedExclusionForce) in the same evaluation */
-#define NBK_ENERGY_FP64 32u /* with NBK_ENERGY: electrostatic pair energies from FP64
-                              geometry and FP64 erfc, summed in FP64 (forces stay FP32).
-                              For energy totals that cancel to a small fraction of
-                              the sum of |pair energies|; about 2-3x slower. */
+#define NBK_ENERGY_FP64 32u /* accepted for compatibility, no effect: electrostatic energies
+                              and the slow virial are always formed in FP64 (see
+                              nbk_nonbonded_force) */
 
 /* ---- POD types -------------------------------------------------------- */
 typedef struct { float x, y, z; } nbk_float3;
@@ -201,7 +200,16 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
  *   d_forcesFixed           : device int64[6*atomStorageSize] SoA
  *                             (fx, fy, fz, fslowx, fslowy, fslowz)
  * With NBK_PAIRLIST the tile lists are refined: masks of pairs within the
- * pairlist cutoff that are not excluded, empty tiles and lists compacted. */
+ * pairlist cutoff that are not excluded, empty tiles and lists compacted.
+ * Precision: pair forces are FP32 (the reference's arithmetic), summed in
+ * fixed point. With NBK_ENERGY the electrostatic (fast and slow) pair
+ * energies, and with NBK_VIRIAL | NBK_SLOW the slow virial, are formed per
+ * interacting pair in FP64 from FP64 geometry (1/r refined by a Newton step,
+ * the slow term from an FP64 piecewise polynomial, nbk_slow_table) and summed
+ * in fixed point: relative error ~1e-12 against an FP64 evaluation of the
+ * same FP32 positions, where FP32 pair energies resolve totals that cancel to
+ * 1e-4 of the sum of |pair energies| only to ~1e-5. The LJ energy (FP32 per
+ * pair) and the fast virial (from the fixed-point forces) hold ~3e-7. */
 NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flags,
                                 nbk_float3 lata, nbk_float3 latb, nbk_float3 latc,
                                 const nbk_float4* xyzq, int xyzqOnDevice, float cutoff2,
@@ -267,8 +275,7 @@ NBK_API int nbk_adjoint(nbk_handle h, unsigned flags, const nbk_float4* d_wF,
  * and its own LJ tables ljA/ljB/ljA14/ljB14 [numReplicas][dim*dim] (dim =
  * params.vdwTableDim). Call after nbk_update_computes; the lattice arguments
  * of later calls are then ignored. Energies, virials and pair counts are kept
- * per replica (nbk_reduce_virial_energy_batch, nbk_get_pair_counts).
- * NBK_ENERGY_FP64 is not available in batched mode. */
+ * per replica (nbk_reduce_virial_energy_batch, nbk_get_pair_counts). */
 NBK_API int nbk_set_replicas(nbk_handle h, int numReplicas, const int* h_replicaOfCompute,
                              const int* h_replicaSlotStart, const nbk_float3* h_lattices,
                              const double* ljA, const double* ljB, const double* ljA14,
@@ -309,6 +316,21 @@ NBK_API int nbk_exclusion_force_noalloc(const nbk_params* params, const float* d
                                         void* stream);
 /* Message of the last failure of nbk_exclusion_force_noalloc on this thread. */
 NBK_API const char* nbk_noalloc_last_error(void);
+
+/* No counterpart in the reference (its slow term comes from interpolated
+ * texture tables, src/CudaNonbondedTables.C:158-303). The FP64 slow-term table
+ * the force kernel's precise pass evaluates. With step D (*step; a power of
+ * two, 2 A^2 or less, chosen so that the fit is within FP64 rounding), row k
+ * (8 doubles) holds the degree-6 Chebyshev interpolant of
+ * phi_s(s) = (3 - s/rc^2)/(2 rc) - erf(ewaldcof sqrt(s))/sqrt(s), s = r^2, on
+ * s in [k D - D/2, k D + D/2], as coefficients c0..c6 of powers of (s - k D),
+ * then a zero. The slow pair energy is qq phi_s(s), the slow force factor
+ * (dE/dr)/r = 2 qq phi_s'(s). Rows cover s up to pairlistdist^2 + 2.
+ * Host-only (no GPU needed): returns the number of rows and, when out is not
+ * NULL, writes them (maxRows must be at least that number); step may be NULL;
+ * NBK_ERR_ARG for bad parameters. */
+NBK_API int nbk_slow_table(double ewaldcof, double cutoff, double pairlistdist, double* out,
+                           int maxRows, double* step);
 
 /* ---- measurement ----------------------------------------------------------- */
 

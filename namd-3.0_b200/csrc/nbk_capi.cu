@@ -75,6 +75,9 @@ struct nbk_context {
   NbkConst64 c64{};
   int ljDim = 0;
   DBuf<float2> ljTable, ljExclTable;
+  DBuf<double2> slowTable;  // FP64 phi_s rows (buildSlowTable)
+  int slowTableRows = 0;
+  double slowStep = 2.0;
   DBuf<unsigned> exclBits;
   int numExclWords = 0;
   // set-up data
@@ -182,58 +185,10 @@ namespace {
 
 float3 f3(nbk_float3 v) { return make_float3(v.x, v.y, v.z); }
 
-void computeConsts(nbk_context* h) {
-  const nbk_params& p = h->prm;
-  NbkConst& c = h->c;
-  const double rc = p.cutoff, rc2 = rc * rc;
-  const double pl2 = p.pairlistdist * p.pairlistdist;
-  const bool sw = p.switchdist < p.cutoff;
-  const double rs2 = sw ? p.switchdist * p.switchdist : rc2;
-  const double c1 = sw ? 1.0 / ((rc2 - rs2) * (rc2 - rs2) * (rc2 - rs2)) : 0.0;
-  c.cutoff2 = (float)rc * (float)rc;
-  c.plcutoff2 = (float)p.pairlistdist * (float)p.pairlistdist;
-  (void)pl2;
-  c.rc2 = (float)rc2;
-  c.rs2 = (float)rs2;
-  c.lj0 = (float)(c1 * (rc2 - 3.0 * rs2));
-  c.lj1 = (float)(2.0 * c1);
-  c.lj2 = (float)(-12.0 * c1);
-  c.lj3 = (float)(12.0 * c1 * rs2);
-  c.rc3inv = (float)(1.0 / (rc * rc2));
-  c.hA = (float)(1.5 / rc);
-  c.hB = (float)(-0.5 / (rc * rc2));
-  c.beta = (float)p.ewaldcof;
-  c.beta2Pi = (float)(2.0 * p.ewaldcof / std::sqrt(M_PI));
-  c.one14 = (float)(1.0 - p.scale14);
-  c.pBeta = (float)(kErfcP * p.ewaldcof);
-  c.gaussK = (float)(-p.ewaldcof * p.ewaldcof / std::log(2.0));
-  c.ljDim = h->ljDim;
-  c.switching = sw ? 1 : 0;
-  c.s0 = sw ? 0.0f : 1.0f;
-  c.hAd = 1.5 / rc;
-  c.hBd = -0.5 / (rc * rc2);
-  c.betad = p.ewaldcof;
-  NbkConst64& k = h->c64;
-  k.rc2 = rc2;
-  k.rs2 = rs2;
-  k.lj0 = c1 * (rc2 - 3.0 * rs2);
-  k.lj1 = 2.0 * c1;
-  k.lj2 = -12.0 * c1;
-  k.lj3 = 12.0 * c1 * rs2;
-  k.rc3inv = 1.0 / (rc * rc2);
-  k.hA = 1.5 / rc;
-  k.hB = -0.5 / (rc * rc2);
-  k.beta = p.ewaldcof;
-  k.beta2Pi = 2.0 * p.ewaldcof / std::sqrt(M_PI);
-  k.one14 = 1.0 - p.scale14;
-  k.switching = sw ? 1 : 0;
-}
-
 // Index of a flag combination in the tuning tables (the force kernel variant).
 int tuneKey(const nbk_context* h, unsigned flags) {
-  const bool E = flags & NBK_ENERGY;
-  return (h->nrep > 0 ? 16 : 0) | (E ? 8 : 0) | ((flags & NBK_VIRIAL) ? 4 : 0) |
-         ((flags & NBK_SLOW) ? 2 : 0) | ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
+  return (h->nrep > 0 ? 8 : 0) | ((flags & NBK_ENERGY) ? 4 : 0) | ((flags & NBK_VIRIAL) ? 2 : 0) |
+         ((flags & NBK_SLOW) ? 1 : 0);
 }
 
 // Force-kernel arguments for the handle's compacted lists, positions, lattice,
@@ -256,7 +211,12 @@ ForceArgs refinedForceArgs(nbk_context* h, float cutoff2) {
   a.stride = h->atomStorageSize;
   a.acc = h->acc.p;
   a.workCounter = h->counters.p + 2;
-  a.c64 = h->c64;
+  a.slowTable = h->slowTable.p;
+  a.slowTableRows = h->slowTableRows;
+  a.slowStep = h->slowStep;
+  a.slowInvStep = 1.0 / h->slowStep;
+  // the precise pass reads the table from shared memory when it is small
+  a.slowTableShared = sizeof(double) * kSlowTableDeg1 * (size_t)h->slowTableRows <= 16 * 1024;
   if (h->nrep > 0) {
     a.compRep = h->compRep.p;
     a.repLat = h->repLat.p;
@@ -270,9 +230,6 @@ ForceArgs refinedForceArgs(nbk_context* h, float cutoff2) {
   a.compF = h->compF;
   return a;
 }
-
-// The FP64 energy mode keeps its per-pair FP64 sums per list: one warp per list.
-bool fp64Energy(unsigned flags) { return (flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64); }
 
 int checkHandle(nbk_handle h, const char* fn) {
   if (!h) return setErr(NBK_ERR_ARG, std::string(fn) + ": NULL handle");
@@ -342,7 +299,7 @@ NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
   h->prm = *p;
   h->prm.ljA = h->prm.ljB = h->prm.ljA14 = h->prm.ljB14 = nullptr;
   h->ljDim = p->vdwTableDim;
-  computeConsts(h);
+  makeConstants(*p, p->vdwTableDim, h->c, h->c64);
   for (int k = 0; k < 32; ++k) {
     h->tuneMinBlocks[k] = 5;
     h->tuneSplitLog2[k] = 0;
@@ -366,6 +323,12 @@ NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
   fin(h->ljExclTable.ensure(dim * dim), "nbk_create: alloc");
   if (rc == NBK_OK) fin(cudaMemcpy(h->ljTable.p, t.data(), sizeof(float2) * t.size(), cudaMemcpyHostToDevice), "nbk_create: copy");
   if (rc == NBK_OK) fin(cudaMemcpy(h->ljExclTable.p, te.data(), sizeof(float2) * te.size(), cudaMemcpyHostToDevice), "nbk_create: copy");
+  // FP64 slow-term table over s in [0, pairlistdist^2 + 2]: the runtime cutoff
+  // can be anything up to the pairlist cutoff
+  std::vector<double> slow;
+  h->slowTableRows = buildSlowTable(p->ewaldcof, p->cutoff, p->pairlistdist, slow, &h->slowStep);
+  fin(h->slowTable.ensure(slow.size() / 2), "nbk_create: alloc");
+  if (rc == NBK_OK) fin(cudaMemcpy(h->slowTable.p, slow.data(), sizeof(double) * slow.size(), cudaMemcpyHostToDevice), "nbk_create: copy");
   fin(h->acc.ensure(kAccCount), "nbk_create: alloc");
   fin(h->counters.ensure(4), "nbk_create: alloc");
   fin(h->ve.ensure(1), "nbk_create: alloc");
@@ -384,6 +347,7 @@ NBK_API int nbk_destroy(nbk_handle h) {
   cudaSetDevice(h->device);
   h->ljTable.release();
   h->ljExclTable.release();
+  h->slowTable.release();
   h->exclBits.release();
   h->computes.release();
   h->vdwTypes.release();
@@ -635,8 +599,6 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   NBK_CUDA(cudaMemsetAsync(h->force.p, 0,
                            sizeof(long long) * 6 * ((size_t)n + (size_t)h->numComputes), st),
            "nbk_nonbonded_force");
-  if (h->nrep > 0 && (flags & NBK_ENERGY_FP64) && (flags & NBK_ENERGY))
-    return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: NBK_ENERGY_FP64 is not available with replicas");
   const int accBlocks = h->nrep > 0 ? h->nrep : 1;
   NBK_CUDA(cudaMemsetAsync(h->acc.p, 0, sizeof(long long) * kAccCount * (size_t)accBlocks, st),
            "nbk_nonbonded_force");
@@ -645,10 +607,10 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   h->latc = f3(latc);
 
   h->lastCutoff2 = cutoff2;
-  const bool shiftVirial = (flags & NBK_VIRIAL) && !fp64Energy(flags);
+  const bool shiftVirial = flags & NBK_VIRIAL;
   ForceArgs a = refinedForceArgs(h, cutoff2);
   const int key = tuneKey(h, flags);
-  a.splitLog2 = fp64Energy(flags) ? 0 : h->tuneSplitLog2[key];
+  a.splitLog2 = h->tuneSplitLog2[key];
   NBK_CUDA(timedEvent(h, true, st), "timing event");
   if (pairlist) {
     // refinement of the culled lists (the pairlist pass), then their
@@ -1069,8 +1031,6 @@ NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* str
   if (!h->refined)
     return setErr(NBK_ERR_STATE, "nbk_autotune: needs refined tile lists (an NBK_PAIRLIST evaluation) first");
   if (flags & ~63u) return setErr(NBK_ERR_ARG, "nbk_autotune: unknown flag bits");
-  if (h->nrep > 0 && (flags & NBK_ENERGY_FP64) && (flags & NBK_ENERGY))
-    return setErr(NBK_ERR_ARG, "nbk_autotune: NBK_ENERGY_FP64 is not available with replicas");
   if (iterations < 1) iterations = 1;
   cudaStream_t st = (cudaStream_t)stream;
   const unsigned kflags = flags & ~(unsigned)(NBK_PAIRLIST | NBK_CORRECTIONS);
@@ -1078,7 +1038,7 @@ NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* str
   const int n = h->atomStorageSize;
   const int accBlocks = h->nrep > 0 ? h->nrep : 1;
   ForceArgs a = refinedForceArgs(h, h->lastCutoff2);
-  const int maxSplitLog2 = fp64Energy(kflags) ? 0 : 2;
+  const int maxSplitLog2 = 2;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   NBK_CUDA(cudaEventCreate(&e0), "nbk_autotune");
   if (cudaEventCreate(&e1) != cudaSuccess) {

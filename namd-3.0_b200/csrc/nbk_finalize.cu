@@ -30,7 +30,13 @@ __device__ __forceinline__ void flushThreadAcc(long long* accBase, int rep, long
   }
 }
 
-template <bool doEnergy, bool doVirial, bool doSlow, bool doE64>
+// Forces are FP32 (fixed-point accumulated, like the nonbonded kernel's);
+// energies and the slow virial are formed per tuple in FP64 from FP64
+// geometry (the shift formed in FP64 from the FP32 offsets and lattice), the
+// same precision as the force kernel's precise pass; the fast virial comes
+// from the forces: the per-atom part in the finalize pass, the shift part
+// F_i (x) shift here.
+template <bool doEnergy, bool doVirial, bool doSlow>
 __global__ void correctionsKernel(const CorrArgs a) {
   const NbkConst& c = a.c;
   const int total = a.numModified + (doSlow ? a.numExcluded : 0);
@@ -81,9 +87,10 @@ __global__ void correctionsKernel(const CorrArgs a) {
     const float rinv2 = rinv * rinv;
     const float rinv3 = rinv * rinv2;
     const float qq = xi.w * xj.w;
-    float g = 0.f, gs = 0.f, eV = 0.f, eE = 0.f, eS = 0.f;
+    float g = 0.f, gs = 0.f;
+    float2 ab = make_float2(0.f, 0.f);
     if (modified) {
-      const float2 ab = ljx[e.vdwtypei * c.ljDim + e.vdwtypej];
+      ab = ljx[e.vdwtypei * c.ljDim + e.vdwtypej];
       const float rinv6 = rinv2 * rinv2 * rinv2;
       const float ab6 = fmaf(ab.x, rinv6, -ab.y);
       const float w = ab6 * rinv6;
@@ -97,17 +104,10 @@ __global__ void correctionsKernel(const CorrArgs a) {
       }
       const float q14 = c.one14 * qq;
       g = fmaf(w, ds, dw * s) - q14 * (c.rc3inv - rinv3);
-      if (doEnergy) {
-        const float h = fmaf(c.hB, r2, c.hA);
-        eV = w * s;
-        eE = -q14 * (rinv - h);
-        if (doSlow) eS = -q14 * h;
-      }
       if (doSlow) gs = q14 * c.rc3inv;
     } else {
       const float r = r2 * rinv;
       const float x = c.beta * r;
-      const float erfx = erff(x);
       // (dE/dr)/r of -qq erf(x)/r is qq (erf(x) - 2/sqrt(pi) x e^{-x^2}) / r^3. The
       // bracket is O(x^3) and cancels badly at excluded-pair distances (O-H:
       // x = 0.25), so below x = 0.5 it is taken from its Taylor series in x^2:
@@ -124,10 +124,9 @@ __global__ void correctionsKernel(const CorrArgs a) {
         q = fmaf(q, y, 2.0f / 3.0f);
         bracket = 1.1283791671f * x * y * q;
       } else {
-        bracket = erfx - c.beta2Pi * r * __expf(-x * x);
+        bracket = erff(x) - c.beta2Pi * r * __expf(-x * x);
       }
       gs = qq * bracket * rinv3;
-      if (doEnergy) eS = -qq * erfx * rinv;
     }
     // F_i += g d, F_j -= g d
     const float fx = g * dx, fy = g * dy, fz = g * dz;
@@ -140,11 +139,9 @@ __global__ void correctionsKernel(const CorrArgs a) {
       atomicAddFixed(&a.force[1 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)qy));
       atomicAddFixed(&a.force[2 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)qz));
     }
-    unsigned long long sx = 0, sy = 0, sz = 0;
     if (doSlow) {
-      sx = toFixedForce(gs * dx);
-      sy = toFixedForce(gs * dy);
-      sz = toFixedForce(gs * dz);
+      const unsigned long long sx = toFixedForce(gs * dx), sy = toFixedForce(gs * dy),
+                               sz = toFixedForce(gs * dz);
       atomicAddFixed(&a.force[3 * (size_t)a.stride + e.i], sx);
       atomicAddFixed(&a.force[4 * (size_t)a.stride + e.i], sy);
       atomicAddFixed(&a.force[5 * (size_t)a.stride + e.i], sz);
@@ -152,8 +149,7 @@ __global__ void correctionsKernel(const CorrArgs a) {
       atomicAddFixed(&a.force[4 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sy));
       atomicAddFixed(&a.force[5 * (size_t)a.stride + e.j], (unsigned long long)(-(long long)sz));
     }
-    if (doE64) {
-      // FP64 mode: energies and the complete pair virial W = -g d (x) d in FP64
+    if (doEnergy || (doVirial && doSlow)) {
       const double S0 = (double)e.ioffsetXYZ.x, S1 = (double)e.ioffsetXYZ.y,
                    S2 = (double)e.ioffsetXYZ.z;
       const double d[3] = {
@@ -161,33 +157,28 @@ __global__ void correctionsKernel(const CorrArgs a) {
           (double)xj.y - ((double)xi.y + (S0 * la.y + S1 * lb.y + S2 * lc.y)),
           (double)xj.z - ((double)xi.z + (S0 * la.z + S1 * lb.z + S2 * lc.z))};
       const double r2d = fma(d[2], d[2], fma(d[1], d[1], d[0] * d[0]));
-      const double ri = rsqrt(r2d), ri2 = ri * ri, ri3 = ri * ri2;
+      const double ri = rsqrt(r2d), ri2 = ri * ri;
       const double qqd = (double)xi.w * (double)xj.w;
       const NbkConst64& k = a.c64;
-      double gd = 0.0, gsd = 0.0, eVd = 0.0, eEd = 0.0, eSd = 0.0;
+      double gsd = 0.0, eVd = 0.0, eEd = 0.0, eSd = 0.0;
       if (modified) {
-        const float2 ab = ljx[e.vdwtypei * c.ljDim + e.vdwtypej];
-        const double ri6 = ri2 * ri2 * ri2;
-        const double ab6 = fma((double)ab.x, ri6, -(double)ab.y);
-        const double w = ab6 * ri6;
-        const double dw = fma((double)ab.x, ri6, ab6) * (-6.0 * ri2 * ri6);
-        double sw = 1.0, dsw = 0.0;
-        if (k.switching) {
-          const double t2 = fmax(r2d, k.rs2), dd = k.rc2 - t2;
-          sw = dd * dd * fma(k.lj1, t2, k.lj0);
-          dsw = dd * fma(k.lj2, t2, k.lj3);
-        }
         const double q14 = k.one14 * qqd, h = fma(k.hB, r2d, k.hA);
-        gd = fma(w, dsw, dw * sw) - q14 * (k.rc3inv - ri3);
-        eVd = w * sw;
-        eEd = -q14 * (ri - h);
-        if (doSlow) {
-          eSd = -q14 * h;
-          gsd = q14 * k.rc3inv;
+        if (doEnergy) {
+          const double ri6 = ri2 * ri2 * ri2;
+          const double w = fma((double)ab.x, ri6, -(double)ab.y) * ri6;
+          double sw = 1.0;
+          if (k.switching) {
+            const double t2 = fmax(r2d, k.rs2), dd = k.rc2 - t2;
+            sw = dd * dd * fma(k.lj1, t2, k.lj0);
+          }
+          eVd = w * sw;
+          eEd = -q14 * (ri - h);
+          if (doSlow) eSd = -q14 * h;
         }
+        if (doSlow) gsd = q14 * k.rc3inv;
       } else {
         const double r = r2d * ri, x = k.beta * r, erfx = erf(x);
-        gsd = qqd * (erfx * ri3 - k.beta2Pi * exp(-x * x) * ri2);
+        gsd = qqd * (erfx * ri2 * ri - k.beta2Pi * exp(-x * x) * ri2);
         eSd = -qqd * erfx * ri;
       }
       if (doEnergy) {
@@ -195,33 +186,20 @@ __global__ void correctionsKernel(const CorrArgs a) {
         acc[kAccEElec] += toFixedEnergy(eEd);
         acc[kAccESlow] += toFixedEnergy(eSd);
       }
-      if (doVirial) {
+      if (doVirial && doSlow) {
 #pragma unroll
-        for (int p = 0; p < 9; ++p) {
-          const double dd = d[p / 3] * d[p % 3];
-          if (modified) acc[kAccVir + p] += toFixedEnergy(-gd * dd);
-          if (doSlow) acc[kAccVirSlow + p] += toFixedEnergy(-gsd * dd);
-        }
+        for (int p = 0; p < 9; ++p) acc[kAccVirSlow + p] += toFixedEnergy(-gsd * (d[p / 3] * d[p % 3]));
       }
-    } else if (doEnergy) {
-      acc[kAccEVdw] += toFixedEnergy((double)eV);
-      acc[kAccEElec] += toFixedEnergy((double)eE);
-      acc[kAccESlow] += toFixedEnergy((double)eS);
     }
-    if (doVirial && !doE64) {
-      // shift part: F_i (x) shift; the per-atom part comes from the finalize pass
+    if (doVirial && modified) {
+      // shift part of the fast virial: F_i (x) shift; the per-atom part comes
+      // from the finalize pass
       const double S[3] = {(double)sh.x, (double)sh.y, (double)sh.z};
       const double Fi[3] = {(double)(long long)qx * kForceScaleInv,
                             (double)(long long)qy * kForceScaleInv,
                             (double)(long long)qz * kForceScaleInv};
-      const double Gi[3] = {(double)(long long)sx * kForceScaleInv,
-                            (double)(long long)sy * kForceScaleInv,
-                            (double)(long long)sz * kForceScaleInv};
 #pragma unroll
-      for (int p = 0; p < 9; ++p) {
-        if (modified) acc[kAccVir + p] += toFixedEnergy(Fi[p / 3] * S[p % 3]);
-        if (doSlow) acc[kAccVirSlow + p] += toFixedEnergy(Gi[p / 3] * S[p % 3]);
-      }
+      for (int p = 0; p < 9; ++p) acc[kAccVir + p] += toFixedEnergy(Fi[p / 3] * S[p % 3]);
     }
   }
   if (doEnergy || doVirial) flushThreadAcc(a.acc, a.slotRep ? curRep : 0, acc);
@@ -229,29 +207,24 @@ __global__ void correctionsKernel(const CorrArgs a) {
 
 cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st) {
   const bool E = flags & NBK_ENERGY, V = flags & NBK_VIRIAL, S = flags & NBK_SLOW;
-  const bool D = E && (flags & NBK_ENERGY_FP64);
   const int total = a.numModified + (S ? a.numExcluded : 0);
   if (total <= 0) return cudaSuccess;
   const int threads = 256;
   const int blocks = min((total + threads - 1) / threads, 2048);
-  const int idx = (D ? 8 : 0) | (E ? 4 : 0) | (V ? 2 : 0) | (S ? 1 : 0);
+  const int idx = (E ? 4 : 0) | (V ? 2 : 0) | (S ? 1 : 0);
   switch (idx) {
-#define NBK_CASE(i, e, v, s, d) \
-  case i:                       \
-    correctionsKernel<e, v, s, d><<<blocks, threads, 0, st>>>(a); \
+#define NBK_CASE(i, e, v, s) \
+  case i:                    \
+    correctionsKernel<e, v, s><<<blocks, threads, 0, st>>>(a); \
     break;
-    NBK_CASE(0, false, false, false, false)
-    NBK_CASE(1, false, false, true, false)
-    NBK_CASE(2, false, true, false, false)
-    NBK_CASE(3, false, true, true, false)
-    NBK_CASE(4, true, false, false, false)
-    NBK_CASE(5, true, false, true, false)
-    NBK_CASE(6, true, true, false, false)
-    NBK_CASE(7, true, true, true, false)
-    NBK_CASE(12, true, false, false, true)
-    NBK_CASE(13, true, false, true, true)
-    NBK_CASE(14, true, true, false, true)
-    NBK_CASE(15, true, true, true, true)
+    NBK_CASE(0, false, false, false)
+    NBK_CASE(1, false, false, true)
+    NBK_CASE(2, false, true, false)
+    NBK_CASE(3, false, true, true)
+    NBK_CASE(4, true, false, false)
+    NBK_CASE(5, true, false, true)
+    NBK_CASE(6, true, true, false)
+    NBK_CASE(7, true, true, true)
 #undef NBK_CASE
   }
   return cudaGetLastError();
@@ -259,10 +232,11 @@ cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st
 
 // Fixed point -> float4 forces (transposeForcesKernel's role,
 // src/CudaComputeNonbondedKernel.cu:2057-2072) and the per-atom part of the
-// virial, sum_i F_i (x) x_i over patch-centred positions
+// fast virial, sum_i F_i (x) x_i over patch-centred positions
 // (reduceNonbondedVirialKernel, :1649-1763), folded into fixed point per atom.
-// Each warp owns a contiguous slot range so that, with batched replicas, its
-// slots belong to one replica except at boundaries.
+// (The slow virial is summed over pairs in FP64 by the force and correction
+// kernels.) Each warp owns a contiguous slot range so that, with batched
+// replicas, its slots belong to one replica except at boundaries.
 constexpr int kFinalizeThreads = 256;
 
 __global__ void __launch_bounds__(kFinalizeThreads)
@@ -272,7 +246,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
                    float4* __restrict__ outSH, int doSlow, int doVirial,
                    long long* __restrict__ accBase, const int* __restrict__ slotRep,
                    const ShiftVirialArgs shift) {
-  long long v[18] = {};
+  long long v[9] = {};
   const int lane = threadIdx.x & 31;
   const int warpsTotal = (gridDim.x * blockDim.x) >> 5;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -287,7 +261,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
       if (__any_sync(0xffffffffu, rep != curRep)) {
         // flush per thread into the replica it accumulated for
 #pragma unroll
-        for (int p = 0; p < 18; ++p) {
+        for (int p = 0; p < 9; ++p) {
           if (v[p] != 0) atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
           v[p] = 0;
         }
@@ -315,12 +289,8 @@ __global__ void __launch_bounds__(kFinalizeThreads)
       const float4 x = xyzq[i];
       const double X[3] = {(double)x.x, (double)x.y, (double)x.z};
       const double Fd[3] = {fx * kForceScaleInv, fy * kForceScaleInv, fz * kForceScaleInv};
-      const double Gd[3] = {gx * kForceScaleInv, gy * kForceScaleInv, gz * kForceScaleInv};
 #pragma unroll
-      for (int p = 0; p < 9; ++p) {
-        v[p] += toFixedEnergy(Fd[p / 3] * X[p % 3]);
-        v[9 + p] += toFixedEnergy(Gd[p / 3] * X[p % 3]);
-      }
+      for (int p = 0; p < 9; ++p) v[p] += toFixedEnergy(Fd[p / 3] * X[p % 3]);
     }
   }
   if (!doVirial) return;
@@ -334,13 +304,13 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     const int rep = shift.compRep ? shift.compRep[c] : 0;
     if (rep != curRep) {
 #pragma unroll
-      for (int p = 0; p < 18; ++p) {
+      for (int p = 0; p < 9; ++p) {
         if (v[p] != 0) atomicAddFixed(&accBase[(size_t)curRep * kAccCount + kAccVir + p], (unsigned long long)v[p]);
         v[p] = 0;
       }
       curRep = rep;
     }
-    const long long* F = shift.compF + 6 * (size_t)c;
+    const long long* Fc = shift.compF + 6 * (size_t)c;
     const nbk_compute_record cr = shift.computes[c];
     float3 la = shift.lata, lb = shift.latb, lc = shift.latc;
     if (shift.compRep) {
@@ -351,22 +321,18 @@ __global__ void __launch_bounds__(kFinalizeThreads)
     const float3 sh = shiftOf(make_float3(cr.offsetXYZ.x, cr.offsetXYZ.y, cr.offsetXYZ.z), la, lb, lc);
     const double S[3] = {(double)sh.x, (double)sh.y, (double)sh.z};
 #pragma unroll
-    for (int p = 0; p < 9; ++p) {
-      v[p] += toFixedEnergy((double)F[p / 3] * kForceScaleInv * S[p % 3]);
-      if (doSlow) v[9 + p] += toFixedEnergy((double)F[3 + p / 3] * kForceScaleInv * S[p % 3]);
-    }
+    for (int p = 0; p < 9; ++p) v[p] += toFixedEnergy((double)Fc[p / 3] * kForceScaleInv * S[p % 3]);
   }
-  // Reduce the warp, then the block, before touching the 18 accumulator
+  // Reduce the warp, then the block, before touching the 9 accumulator
   // words: every block adds each word once (per-warp adds only where a block
   // spans two replicas), which keeps same-address atomics off the critical path.
-  __shared__ long long s_v[kFinalizeThreads / 32][18];
+  __shared__ long long s_v[kFinalizeThreads / 32][9];
   __shared__ int s_rep[kFinalizeThreads / 32];
   const int wib = threadIdx.x >> 5;
   const int rep0 = __shfl_sync(0xffffffffu, curRep, 0);
   const bool uniform = __all_sync(0xffffffffu, curRep == rep0);
 #pragma unroll
-  for (int p = 0; p < 18; ++p) {
-    if (p >= 9 && !doSlow) break;
+  for (int p = 0; p < 9; ++p) {
     if (uniform) {
       const long long sw = warpSumLL(v[p]);
       if (lane == 0) s_v[wib][p] = sw;
@@ -378,7 +344,7 @@ __global__ void __launch_bounds__(kFinalizeThreads)
   if (lane == 0) s_rep[wib] = uniform ? rep0 : -1;
   __syncthreads();
   const int nw = blockDim.x >> 5;
-  if (threadIdx.x < 18 && (threadIdx.x < 9 || doSlow)) {
+  if (threadIdx.x < 9) {
     const int p = threadIdx.x;
     bool same = true;
     for (int w = 1; w < nw; ++w) same = same && (s_rep[w] == s_rep[0] || s_rep[w] < 0);
@@ -406,14 +372,10 @@ cudaError_t launchFinalizeForces(int n, const long long* force, int stride, cons
   // two blocks per SM keep enough loads in flight (one per SM left the
   // kernel latency-bound: 11 -> 9 us at 97k slots)
   const int blocks = min((n + threads - 1) / threads, 2 * numSM);
-  // the FP64 energy/virial mode accumulates complete pair virials instead
-  const bool atomVirial = V && !((flags & NBK_ENERGY) && (flags & NBK_ENERGY_FP64));
-  if (!atomVirial && !outF && !outS && !outFHost && !outSHost) return cudaSuccess;
   ShiftVirialArgs sv{};
-  if (shift && atomVirial) sv = *shift;
+  if (shift && V) sv = *shift;
   finalizeKernel<<<blocks, threads, 0, st>>>(n, force, stride, xyzq, outF, outS, outFHost,
-                                             outSHost,
-                                             (flags & NBK_SLOW) ? 1 : 0, atomVirial ? 1 : 0, acc,
+                                             outSHost, (flags & NBK_SLOW) ? 1 : 0, V ? 1 : 0, acc,
                                              slotRep, sv);
   return cudaGetLastError();
 }

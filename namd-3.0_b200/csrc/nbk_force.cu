@@ -3,105 +3,326 @@
 // One warp owns one tile list (32 i atoms of one patch against the j tiles of
 // a compute's partner patch), as CudaComputeNonbondedKernel's
 // nonbondedForceKernel does (src/CudaComputeNonbondedKernel.cu:629-1644), but:
-//   - j forces ride in registers and rotate one lane per step with a shuffle
-//     (lane l works on j = (l+t) & 31 at step t), so the inner loop touches
-//     shared memory only for the broadcast-free j coordinate load;
-//   - steps whose bit is clear in every lane's mask are skipped warp-uniformly
-//     (the rotation jumps by the step distance);
+//   - two pair steps per iteration run through sm_100's packed FP32
+//     instructions; j forces ride in registers and rotate with a shuffle, so
+//     the inner loop touches shared memory only for the j-tile loads;
+//   - steps whose bit is clear in every lane's mask are skipped warp-uniformly;
 //   - the lists it reads are already refined (TileExcl masks from
 //     refineKernel); a pairlist step refines, compacts, then runs this kernel;
 //   - per-tile FP32 partial forces are folded into 64-bit fixed point with
 //     integer atomics, so the summed forces do not depend on the order in
-//     which lists run; energies and virials are folded into fixed point per
-//     list for the same reason.
+//     which lists run;
+//   - on energy and virial evaluations the electrostatic energies and the
+//     slow virial are formed in FP64 by a precise pass over the tile's
+//     interacting pairs, compacted into a queue (see precisePass), and folded
+//     into fixed point per tile; the LJ energy is summed in FP32 per group of
+//     tiles and the fast virial comes from the fixed-point forces.
 #include "nbk_internal.cuh"
 #include "nbk_launch.h"
+
+#include <mutex>
 
 namespace nbk {
 
 constexpr int kForceWarps = 4;
-// FP32 mode: i-force and energy partials are folded into fixed point once per
-// group of kFoldTiles j tiles (groups counted from the start of the list; a
-// list's parts hold whole groups), so every sum is independent of the split.
+// Forces and the LJ energy are folded into fixed point once per group of
+// kFoldTiles j tiles (groups counted from the start of the list; a list's
+// parts hold whole groups), so every sum is independent of the split.
 constexpr int kFoldTiles = 4;
 constexpr int kForceThreads = kForceWarps * kWarp;
 
+// FP64 quantities of the precise pass; after a tile's pass lane q < kNumQ
+// holds quantity q: the fast and slow electrostatic energies, then the six
+// independent components of the slow virial (xx, xy, xz, yy, yz, zz).
+constexpr int kQElec = 0, kQSlow = 1, kQVir = 2, kNumQ = 8;
 
-// Adds a warp's fixed-point accumulators to one replica's accumulator block.
-template <bool doEnergy, bool doVirial>
-__device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& accE0,
-                                          long long& accE1, long long& accE2, long long& accVir,
-                                          int& npair) {
-  if (doVirial && lane < 18 && accVir != 0)
-    atomicAddFixed(&acc[kAccVir + lane], (unsigned long long)accVir);
-  if (doEnergy && lane == 0) {
-    if (accE0) atomicAddFixed(&acc[kAccEVdw], (unsigned long long)accE0);
-    if (accE1) atomicAddFixed(&acc[kAccEElec], (unsigned long long)accE1);
-    if (accE2) atomicAddFixed(&acc[kAccESlow], (unsigned long long)accE2);
+// An atom in FP64 (position, scaled charge); 32 bytes, two 16-byte loads.
+struct alignas(16) Atom64 {
+  double x, y, z, q;
+};
+
+// virialSlow[3a+b] slots of symmetric component m (xx, xy, xz, yy, yz, zz);
+// s1 < 0 for the diagonal.
+__device__ __forceinline__ void symSlots(int m, int& s0, int& s1) {
+  s0 = m == 0 ? 0 : m == 1 ? 1 : m == 2 ? 2 : m == 3 ? 4 : m == 4 ? 5 : 8;
+  s1 = m == 1 ? 3 : m == 2 ? 6 : m == 4 ? 7 : -1;
+}
+
+// Adds a warp's fixed-point accumulators to one replica's accumulator block:
+// lane 0 the LJ energy (accVdw) and, with the other lanes, the pair count;
+// lane q < kNumQ its precise-pass quantity (accQ).
+template <bool doEnergy>
+__device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& accVdw,
+                                          long long& accQ, int& npair) {
+  if (lane < kNumQ && accQ != 0) {
+    if (lane == kQElec) {
+      atomicAddFixed(&acc[kAccEElec], (unsigned long long)accQ);
+    } else if (lane == kQSlow) {
+      atomicAddFixed(&acc[kAccESlow], (unsigned long long)accQ);
+    } else {
+      int s0, s1;
+      symSlots(lane - kQVir, s0, s1);
+      atomicAddFixed(&acc[kAccVirSlow + s0], (unsigned long long)accQ);
+      if (s1 >= 0) atomicAddFixed(&acc[kAccVirSlow + s1], (unsigned long long)accQ);
+    }
   }
   if (doEnergy) {
+    if (lane == 0 && accVdw != 0) atomicAddFixed(&acc[kAccEVdw], (unsigned long long)accVdw);
     int s = npair;
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0 && s) atomicAddFixed(&acc[kAccNumPairs], (unsigned long long)s);
   }
-  accE0 = accE1 = accE2 = accVir = 0;
+  accVdw = accQ = 0;
   npair = 0;
+}
+
+// FP64 geometry of one queued pair: d = x_j - x_i and the charge product.
+struct PairTerms {
+  double dx, dy, dz, qq;
+};
+
+// One lane's precise-pass sums over the current tile group.
+struct LaneSums {
+  double eE, eS, w0, w1, w2, w3, w4, w5;
+};
+
+// The slow-term table as the precise pass reads it: in shared memory,
+// coefficient n of row k at sh[n * rows + k] (a warp's lanes read one
+// coefficient of up to 32 rows per load, few bank conflicts), or else the
+// global row-major copy (8 doubles per row).
+struct SlowTable {
+  const double* sh;
+  const double2* gl;
+  int rows;
+  unsigned last;
+  double step, invStep;
+};
+
+// The FP64 terms of one interacting pair (qq = 0 contributes exact zeros):
+// the fast energy qq (1/r - h(s)) with 1/r from the FP32 approximation
+// refined by one Newton step, and from the slow-term table the slow energy
+// qq phi_s(s) and the slow virial -2 qq phi_s'(s) d (x) d.
+template <bool doEnergy, bool doVirial, bool doSlow>
+__device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable& T,
+                                            const NbkConst& c, LaneSums& L) {
+  const double s = fma(u.dz, u.dz, fma(u.dy, u.dy, u.dx * u.dx));
+  double p = 0.0, dp = 0.0;
+  if (doSlow) {
+    // row k = nearest integer to s/D: adding 1.5 * 2^52 rounds s/D (exact, D
+    // a power of two) into the low word; the sum is clamped to the last row
+    // in FP64, so k and w = s - k D come without an integer conversion
+    const double magic = 6755399441055744.0;
+    const double t = fmin(fma(s, T.invStep, magic), magic + (double)T.last);
+    const unsigned k = (unsigned)__double2loint(t);
+    const double wq = fma(-T.step, t - magic, s);
+    double c0, c1, c2, c3, c4, c5, c6;
+    if (T.sh) {
+      const double* col = T.sh + k;
+      c0 = col[0];
+      c1 = col[T.rows];
+      c2 = col[2 * T.rows];
+      c3 = col[3 * T.rows];
+      c4 = col[4 * T.rows];
+      c5 = col[5 * T.rows];
+      c6 = col[6 * T.rows];
+    } else {
+      const double2* row = T.gl + (size_t)k * (kSlowTableRow / 2);
+      const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2),
+                    c67 = __ldg(row + 3);
+      c0 = c01.x, c1 = c01.y, c2 = c23.x, c3 = c23.y, c4 = c45.x, c5 = c45.y, c6 = c67.x;
+    }
+    // Horner for p(w) and p'(w) together
+    p = c6;
+    dp = p;
+    p = fma(p, wq, c5);
+    dp = fma(dp, wq, p);
+    p = fma(p, wq, c4);
+    dp = fma(dp, wq, p);
+    p = fma(p, wq, c3);
+    dp = fma(dp, wq, p);
+    p = fma(p, wq, c2);
+    dp = fma(dp, wq, p);
+    p = fma(p, wq, c1);
+    dp = fma(dp, wq, p);
+    p = fma(p, wq, c0);
+  }
+  if (doEnergy) {
+    // y0 has relative error below 2^-22; after the step, below 2^-43
+    const double y0 = (double)rsqrtApprox((float)s);
+    const double hs = 0.5 * s;
+    const double y = fma(y0, fma(-hs * y0, y0, 0.5), y0);
+    L.eE = fma(u.qq, y - fma(c.hBd, s, c.hAd), L.eE);
+    if (doSlow) L.eS = fma(u.qq, p, L.eS);
+  }
+  if (doVirial && doSlow) {
+    const double g = (u.qq + u.qq) * dp;  // (dE/dr)/r
+    const double gx = -g * u.dx, gy = -g * u.dy, gz = -g * u.dz;
+    L.w0 = fma(gx, u.dx, L.w0);
+    L.w1 = fma(gx, u.dy, L.w1);
+    L.w2 = fma(gx, u.dz, L.w2);
+    L.w3 = fma(gy, u.dy, L.w3);
+    L.w4 = fma(gy, u.dz, L.w4);
+    L.w5 = fma(gz, u.dz, L.w5);
+  }
+}
+
+// The precise pass of one tile. live (per lane): bit t set when the pair
+// (i = lane, j = (lane + t) & 31) is an interacting pair (mask bit set and
+// FP32 r^2 below the cutoff, the classification the FP32 math used). The
+// warp compacts the tile's interacting pairs into a queue in shared memory
+// (entry = i | t << 5, lane-major order; at most 32 * 32 two-byte entries,
+// the 2 KB of pq) and processes them in FP64, two per lane per iteration
+// (entries e and e + 32: independent dependency chains; an entry past the
+// end gets d = (1, 0, 0) and qq = 0, which contributes exact zeros -- its
+// atoms may be one and the same atom, so their own distance, 0, would turn
+// the zero into a NaN), adding to the lane's group sums L. Every step is
+// warp-synchronous and the sums depend only on the tile group.
+template <bool doEnergy, bool doVirial, bool doSlow>
+__device__ __forceinline__ void precisePass(const unsigned live, const int lane,
+                                            const Atom64* __restrict__ ai,
+                                            const Atom64* __restrict__ aj, double* pq,
+                                            const SlowTable& T, const NbkConst& c, LaneSums& L,
+                                            int& npair) {
+  const int n = __popc(live);
+  if (doEnergy) npair += n;
+  int incl = n;
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
+  if (total == 0) return;  // warp-uniform
+  unsigned short* q = reinterpret_cast<unsigned short*>(pq);
+  int pos = incl - n;
+  for (unsigned w = live; w; w &= w - 1) q[pos++] = (unsigned short)(lane | ((__ffs(w) - 1) << 5));
+  __syncwarp();
+  for (int base = 0; base < total; base += 2 * kWarp) {  // warp-uniform
+    PairTerms u[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int e = base + h * kWarp + lane;
+      if (e < total) {
+        const unsigned ent = q[e];
+        const int i = ent & 31, j = (i + (ent >> 5)) & 31;
+        const Atom64 A = ai[i], B = aj[j];
+        u[h].dx = B.x - A.x;
+        u[h].dy = B.y - A.y;
+        u[h].dz = B.z - A.z;
+        u[h].qq = A.q * B.q;
+      } else {
+        u[h].dx = 1.0;
+        u[h].dy = u[h].dz = u[h].qq = 0.0;
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) precisePair<doEnergy, doVirial, doSlow>(u[h], T, c, L);
+  }
+  __syncwarp();  // the queue is consumed before pq is written again
+}
+
+// End of a tile group: each lane's sums are written to shared memory (pq,
+// [kNumQ][32]) and reduced per quantity in a fixed order (lane L sums
+// quantity L & 7 over lanes 8 (L >> 3) .. 8 (L >> 3) + 7, then two butterfly
+// steps combine the four groups), and lane q < kNumQ adds quantity q, in
+// fixed point, to accQ; the sums restart at zero.
+__device__ __forceinline__ void reduceGroup(const int lane, double* pq, LaneSums& L,
+                                            long long& accQ) {
+  pq[kQElec * kWarp + lane] = L.eE;
+  pq[kQSlow * kWarp + lane] = L.eS;
+  pq[(kQVir + 0) * kWarp + lane] = L.w0;
+  pq[(kQVir + 1) * kWarp + lane] = L.w1;
+  pq[(kQVir + 2) * kWarp + lane] = L.w2;
+  pq[(kQVir + 3) * kWarp + lane] = L.w3;
+  pq[(kQVir + 4) * kWarp + lane] = L.w4;
+  pq[(kQVir + 5) * kWarp + lane] = L.w5;
+  __syncwarp();
+  const double* src = pq + (lane & 7) * kWarp + (lane >> 3) * 8;
+  double v = src[0];
+#pragma unroll
+  for (int m = 1; m < 8; ++m) v += src[m];
+  v += __shfl_xor_sync(0xffffffffu, v, 8);
+  v += __shfl_xor_sync(0xffffffffu, v, 16);
+  if (lane < kNumQ) accQ += toFixedEnergy(v);
+  L = LaneSums{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  __syncwarp();  // pq is free for the next tile's queue
 }
 
 // MINB: CTAs per SM the register budget is cut for (4, 5 or 6 -> 128, 96 or
 // 80 registers; the packed loop holds two pairs' state, and 5 is the untuned
 // default); a.splitLog2: each list's j tiles are shared by 2^splitLog2
 // work items (warps), contiguous parts of equal tile count. Both are launch
-// choices of the autotuner; results do not depend on them (fixed-point sums).
-template <bool doEnergy, bool doVirial, bool doSlow, bool doE64, bool doBatch, int MINB>
+// choices of the autotuner; results do not depend on them (fixed-point sums
+// per tile group, precise-pass sums per tile).
+template <bool doEnergy, bool doVirial, bool doSlow, bool doBatch, int MINB>
 __global__ void __launch_bounds__(kForceThreads, MINB)
     forceKernel(const __grid_constant__ ForceArgs a) {
-  extern __shared__ float2 s_lj[];  // [ljDim*ljDim]
-  __shared__ float4 s_xyzq[kForceWarps][kWarp];
-  // packed loop: the j tile as five rows (x, y, z, q, type bits) of 64
-  // entries; entry m holds the values of atoms m & 31 and (m & 31) ^ 16, so
-  // that the two packed elements of iteration k, j = (lane + k) & 31 and
-  // j ^ 16, come from one 8-byte load at the fixed offset lane + k
+  // the precise pass runs on energy evaluations and on virial evaluations
+  // with slow forces (it forms the slow virial)
+  constexpr bool kPrecise = doEnergy || (doVirial && doSlow);
+  constexpr int kPW = kPrecise ? kForceWarps : 1;
+  // dynamic: the LJ table [ljDim*ljDim] (single system), then, when it fits,
+  // the slow-term table in its transposed layout [7][rows] (precise pass)
+  extern __shared__ float2 s_lj[];
+  // the j tile as five rows (x, y, z, q, type bits) of 64 entries; entry m
+  // holds the values of atoms m & 31 and (m & 31) ^ 16, so that the two
+  // packed elements of iteration k, j = (lane + k) & 31 and j ^ 16, come from
+  // one 8-byte load at the fixed offset lane + k
   __shared__ float2 s_jt[kForceWarps][5][2 * kWarp];
-  __shared__ int s_type[kForceWarps][kWarp];
-  // FP32 mode: each lane's i force of the current list part in fixed point,
-  // folded in at the end of every j tile, so that the sums do not depend on
-  // how a list's tiles are split among warps
+  // each lane's i force of the current list part in fixed point, folded in
+  // at the end of every tile group, so that the sums do not depend on how a
+  // list's tiles are split among warps
   __shared__ long long s_fi[kForceWarps][6][kWarp];
-  // FP32 mode: each lane's energies of the current list part in fixed point
-  // (s_eq) and of the current tile group in FP32 (s_eg), and the warp's
-  // fixed-point energy totals (s_acc, lane 0), kept in shared memory rather
-  // than in registers the pair loop needs
-  __shared__ long long s_eq[kForceWarps][3][kWarp];
-  __shared__ float s_eg[kForceWarps][3][kWarp];
-  __shared__ long long s_acc[kForceWarps][3];
+  // each lane's LJ energy of the list part in fixed point (s_ev) and of the
+  // current tile group in FP32 (s_evg), and the warp's fixed-point LJ total
+  // (s_evw, lane 0), kept in shared memory rather than in registers the pair
+  // loop needs
+  __shared__ long long s_ev[kForceWarps][kWarp];
+  __shared__ float s_evg[kForceWarps][kWarp];
+  __shared__ long long s_evw[kForceWarps];
+  // precise pass: FP64 shifted i atoms of the list, FP64 j atoms of the tile,
+  // and the pair queue / lane partials (2 KB per warp)
+  __shared__ Atom64 s_ai[kPW][kWarp];
+  __shared__ Atom64 s_aj[kPW][kWarp];
+  __shared__ double s_pq[kPW][kNumQ * kWarp];
 
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const NbkConst& c = a.c;
   const int dim = c.ljDim;
-  if (!doBatch) {
-    for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) s_lj[k] = a.ljTable[k];
-    __syncthreads();
+  const int ljWords = doBatch ? 0 : dim * dim;
+  SlowTable T;
+  T.rows = a.slowTableRows;
+  T.last = (unsigned)(a.slowTableRows - 1);
+  T.step = a.slowStep;
+  T.invStep = a.slowInvStep;
+  T.gl = a.slowTable;
+  T.sh = nullptr;
+  if (!doBatch)
+    for (int k = threadIdx.x; k < ljWords; k += blockDim.x) s_lj[k] = a.ljTable[k];
+  if (kPrecise && doSlow && a.slowTableShared) {
+    double* st = reinterpret_cast<double*>(s_lj + ljWords);
+    const double* g = reinterpret_cast<const double*>(a.slowTable);
+    for (int k = threadIdx.x; k < kSlowTableDeg1 * T.rows; k += blockDim.x) {
+      const int n = k / T.rows, r = k - n * T.rows;
+      st[k] = g[(size_t)r * kSlowTableRow + n];
+    }
+    T.sh = st;
   }
+  if (!doBatch || (kPrecise && doSlow && a.slowTableShared)) __syncthreads();
 
   const int numLists = a.numListsDev ? *a.numListsDev : a.numListsHost;
 
-  // per-warp fixed-point accumulators: lane k < 9 owns virial[k], 9 <= k < 18
-  // owns virialSlow[k-9]; lane 0 also owns the three energies.
-  long long accE0 = 0, accE1 = 0, accE2 = 0, accVir = 0;
-  int npair = 0;
-  if (!doE64) {
+  long long accVdw = 0;  // lane 0: LJ energy to flush (batched replica change)
+  long long accQ = 0;    // lane q < kNumQ: precise-pass quantity q
+  LaneSums lsum{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this lane's precise-pass group sums
+  int npair = 0;         // interacting pairs counted by this lane (energy evaluations)
 #pragma unroll
-    for (int q = 0; q < 6; ++q) s_fi[wib][q][lane] = 0;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      s_eq[wib][q][lane] = 0;
-      s_eg[wib][q][lane] = 0.f;
-    }
-    if (lane < 3) s_acc[wib][lane] = 0;
-  }  // interacting pairs seen by this lane (energy evaluations)
+  for (int q = 0; q < 6; ++q) s_fi[wib][q][lane] = 0;
+  s_ev[wib][lane] = 0;
+  s_evg[wib][lane] = 0.f;
+  if (lane == 0) s_evw[wib] = 0;
   int curRep = 0;  // replica whose accumulators the warp is holding
 
   // lists are handed out one at a time from a global counter, so warps that
@@ -125,14 +346,11 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     if (doBatch) {
       const int rep = __ldg(&a.compRep[tl.icompute]);
       if (rep != curRep) {
-        if (!doE64 && lane == 0) {
-          accE0 = s_acc[wib][0];
-          accE1 = s_acc[wib][1];
-          accE2 = s_acc[wib][2];
-          s_acc[wib][0] = s_acc[wib][1] = s_acc[wib][2] = 0;
+        if (lane == 0) {
+          accVdw = s_evw[wib];
+          s_evw[wib] = 0;
         }
-        flushWarp<doEnergy, doVirial>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1,
-                                      accE2, accVir, npair);
+        flushWarp<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accVdw, accQ, npair);
         curRep = rep;
       }
       la = a.repLat[3 * rep];
@@ -146,33 +364,35 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
 
     const int iatom = tl.iatomStart + lane;
     float4 xi = a.xyzq[iatom];
-    // FP64 shifted i position (FP64 energy mode): the shift is formed in FP64
-    // from the FP32 offsets and lattice, without the FP32 rounding of sh
-    double xid = 0.0, yid = 0.0, zid = 0.0;
-    if (doE64) {
-      xid = (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x);
-      yid = (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y);
-      zid = (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z);
+    if (kPrecise) {
+      // FP64 shifted i atom: the shift formed in FP64 from the FP32 offsets
+      // and lattice (the exact lattice translation), without the FP32
+      // rounding of sh
+      const double sx = (double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x;
+      const double sy = (double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y;
+      const double sz = (double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z;
+      Atom64 ai;
+      ai.x = (double)xi.x + sx;
+      ai.y = (double)xi.y + sy;
+      ai.z = (double)xi.z + sz;
+      ai.q = (double)xi.w;
+      s_ai[wib][lane] = ai;
     }
     xi.x = __fadd_rn(xi.x, sh.x);
     xi.y = __fadd_rn(xi.y, sh.y);
     xi.z = __fadd_rn(xi.z, sh.z);
     const int ti = a.vdwTypes[iatom] * dim;
 
-    float fix = 0.f, fiy = 0.f, fiz = 0.f, fisx = 0.f, fisy = 0.f, fisz = 0.f;
-    // packed loop: this tile's two partial i sums per component
+    // this tile group's two partial i sums per component
     float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
     float2 fisx2 = f2(0.f), fisy2 = f2(0.f), fisz2 = f2(0.f);
-    double eV = 0.0, eE = 0.0, eS = 0.0;         // FP64 energy mode, per list
-    double wv[6] = {0, 0, 0, 0, 0, 0}, ws[6] = {0, 0, 0, 0, 0, 0};  // FP64 pair virials
 
     for (int jt = jtFirst; jt <= jtLast; ++jt) {
       const int jstart = a.tileJatomStart[jt];
       const unsigned mask = a.tileExcls[jt].excl[lane];
-      unsigned stepMask = __reduce_or_sync(0xffffffffu, mask);
-      if (stepMask == 0) continue;
-      const float4 xj = a.xyzq[jstart + lane];
-      if constexpr (!doE64) {
+      const unsigned stepMask = __reduce_or_sync(0xffffffffu, mask);
+      if (stepMask != 0) {
+        const float4 xj = a.xyzq[jstart + lane];
         const float tyj = __int_as_float(a.vdwTypes[jstart + lane]);
         // entry m holds (atom m & 31, atom (m & 31) ^ 16): one 8-byte load
         // gives both packed elements of an iteration
@@ -186,27 +406,27 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
         s_jt[wib][2][lane] = s_jt[wib][2][lane + kWarp] = ez;
         s_jt[wib][3][lane] = s_jt[wib][3][lane + kWarp] = eq;
         s_jt[wib][4][lane] = s_jt[wib][4][lane + kWarp] = et;
-      } else {
-        s_xyzq[wib][lane] = xj;
-      }
-      s_type[wib][lane] = a.vdwTypes[jstart + lane];
-      __syncwarp();
+        if (kPrecise) {
+          Atom64 aj;
+          aj.x = (double)xj.x;
+          aj.y = (double)xj.y;
+          aj.z = (double)xj.z;
+          aj.q = (double)xj.w;
+          s_aj[wib][lane] = aj;
+        }
+        __syncwarp();
 
-      float fjx = 0.f, fjy = 0.f, fjz = 0.f, fjsx = 0.f, fjsy = 0.f, fjsz = 0.f;
-      float eVt = 0.f, eEt = 0.f, eSt = 0.f;
-      if constexpr (!doE64) {
-        // Iteration k takes steps k and k+16 together through
-        // the packed FP32 math (element x = step k, element y = step k+16);
-        // iterations whose two steps are clear in every lane are skipped.
-        // i forces keep two partial sums (x, y), folded at the end of the
-        // list. j forces keep two accumulator sets: P follows step k, Q step
-        // k+16, so both rotate by the same amount; they are folded at the
-        // end of the tile.
+        // Iteration k takes steps k and k+16 together through the packed
+        // FP32 math (element x = step k, element y = step k+16); iterations
+        // whose two steps are clear in every lane are skipped. j forces keep
+        // two accumulator sets: P follows step k, Q step k+16, so both rotate
+        // by the same amount; they are folded at the end of the tile.
         float2 PQx = f2(0.f), PQy = f2(0.f), PQz = f2(0.f);     // (P, Q) fast
         float2 PQsx = f2(0.f), PQsy = f2(0.f), PQsz = f2(0.f);  // (P, Q) slow
-        float2 eV2 = f2(0.f), eE2 = f2(0.f), eS2 = f2(0.f);
+        float2 eV2 = f2(0.f);
         const float2 nXi = f2(-xi.x), nYi = f2(-xi.y), nZi = f2(-xi.z);
         int kLast = 0;
+        unsigned live = 0;   // precise pass: interacting pairs, TileExcl bit order
         unsigned mk = mask;  // bit k of the mask moved to bit 0 (and k+16 to 16)
 #pragma unroll 2
         for (int k = 0; k < 16; ++k, mk >>= 1) {
@@ -221,7 +441,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
           const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
           if (!__any_sync(0xffffffffu, aA || aB)) continue;
-          if (doEnergy) npair += (int)aA + (int)aB;
+          if (kPrecise) live |= ((aA ? 1u : 0u) | (aB ? 0x10000u : 0u)) << k;
           const float2 TY = pA[256];
           const int tyA = __float_as_int(TY.x), tyB = __float_as_int(TY.y);
           const float2 abA = doBatch ? __ldg(&ljRow[ti + tyA]) : s_lj[ti + tyA];
@@ -232,7 +452,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           const float2 As = make_float2(aA ? abA.x : 0.f, aB ? abB.x : 0.f);
           const float2 nBs = make_float2(aA ? -abA.y : 0.f, aB ? -abB.y : 0.f);
           float2 F, FS;
-          pairForce2<doEnergy, doSlow>(r2s, qqs, As, nBs, c, F, FS, eV2, eE2, eS2);
+          pairForce2<doEnergy, doSlow>(r2s, qqs, As, nBs, c, F, FS, eV2);
           // i: two partial sums; inactive elements add exact zeros
           fix2 = fma2(DX, F, fix2);
           fiy2 = fma2(DY, F, fiy2);
@@ -264,6 +484,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           }
         }
         // rotate P (at step kLast) and Q (at step kLast+16) back to j = lane
+        float fjx, fjy, fjz, fjsx = 0.f, fjsy = 0.f, fjsz = 0.f;
         {
           const int srcP = (lane + 32 - kLast) & 31, srcQ = (lane + 16 - kLast) & 31;
           fjx = __shfl_sync(0xffffffffu, PQx.x, srcP) + __shfl_sync(0xffffffffu, PQx.y, srcQ);
@@ -275,120 +496,29 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
             fjsz = __shfl_sync(0xffffffffu, PQsz.x, srcP) + __shfl_sync(0xffffffffu, PQsz.y, srcQ);
           }
         }
-        eVt = eV2.x + eV2.y;
-        eEt = eE2.x + eE2.y;
-        eSt = eS2.x + eS2.y;
-      } else {
-        int tPrev = 0;
-        while (stepMask) {
-          const int t = __ffs(stepMask) - 1;
-          stepMask &= stepMask - 1;
-          // rotate the j accumulators so this lane holds those of j = (lane+t)&31
-          const int delta = t - tPrev;
-          if (delta) {
-            const int src = (lane + delta) & 31;
-            fjx = __shfl_sync(0xffffffffu, fjx, src);
-            fjy = __shfl_sync(0xffffffffu, fjy, src);
-            fjz = __shfl_sync(0xffffffffu, fjz, src);
-            if (doSlow) {
-              fjsx = __shfl_sync(0xffffffffu, fjsx, src);
-              fjsy = __shfl_sync(0xffffffffu, fjsy, src);
-              fjsz = __shfl_sync(0xffffffffu, fjsz, src);
-            }
-          }
-          tPrev = t;
-          const int j = (lane + t) & 31;
-          const float4 xjj = s_xyzq[wib][j];
-          const float dx = __fsub_rn(xjj.x, xi.x);
-          const float dy = __fsub_rn(xjj.y, xi.y);
-          const float dz = __fsub_rn(xjj.z, xi.z);
-          const float r2 = dist2(dx, dy, dz);
-          if (((mask >> t) & 1u) && (r2 < c.cutoff2)) {
-            if (doEnergy) ++npair;
-            const float2 ab = doBatch ? __ldg(&ljRow[ti + s_type[wib][j]]) : s_lj[ti + s_type[wib][j]];
-            float f, fs;
-            pairForce<doEnergy, doSlow>(r2, xi.w * xjj.w, ab, c, f, fs, eVt, eEt, eSt);
-            if (doE64) {
-              // electrostatic energies and the pair virials again in FP64 from
-              // FP64 geometry; the FP32 eEt/eSt are discarded in this mode
-              const double ex = (double)xjj.x - xid, ey = (double)xjj.y - yid,
-                           ez = (double)xjj.z - zid;
-              const double r2d = fma(ez, ez, fma(ey, ey, ex * ex));
-              double g, gs;
-              pairFP64<doSlow>(r2d, (double)xi.w * (double)xjj.w, (double)ab.x, (double)ab.y,
-                               a.c64, g, gs, eE, eS);
-              if (doVirial) {
-                const double d[3] = {ex, ey, ez};
-  #pragma unroll
-                for (int u = 0, q = 0; u < 3; ++u)
-  #pragma unroll
-                  for (int v = u; v < 3; ++v, ++q) {
-                    const double dd = d[u] * d[v];
-                    wv[q] = fma(-g, dd, wv[q]);
-                    if (doSlow) ws[q] = fma(-gs, dd, ws[q]);
-                  }
-              }
-            }
-            const float fx = dx * f, fy = dy * f, fz = dz * f;
-            fix += fx;
-            fiy += fy;
-            fiz += fz;
-            fjx -= fx;
-            fjy -= fy;
-            fjz -= fz;
-            if (doSlow) {
-              const float sx = dx * fs, sy = dy * fs, sz = dz * fs;
-              fisx += sx;
-              fisy += sy;
-              fisz += sz;
-              fjsx -= sx;
-              fjsy -= sy;
-              fjsz -= sz;
-            }
-          }
+        const int jatom = jstart + lane;
+        if (fjx != 0.f || fjy != 0.f || fjz != 0.f) {
+          atomicAddFixed(&a.force[0 * (size_t)a.stride + jatom], toFixedForce(fjx));
+          atomicAddFixed(&a.force[1 * (size_t)a.stride + jatom], toFixedForce(fjy));
+          atomicAddFixed(&a.force[2 * (size_t)a.stride + jatom], toFixedForce(fjz));
         }
-        // final rotation: lane l holds the accumulators of j = l again
-        {
-          const int src = (lane + (32 - tPrev)) & 31;
-          fjx = __shfl_sync(0xffffffffu, fjx, src);
-          fjy = __shfl_sync(0xffffffffu, fjy, src);
-          fjz = __shfl_sync(0xffffffffu, fjz, src);
-          if (doSlow) {
-            fjsx = __shfl_sync(0xffffffffu, fjsx, src);
-            fjsy = __shfl_sync(0xffffffffu, fjsy, src);
-            fjsz = __shfl_sync(0xffffffffu, fjsz, src);
-          }
+        if (doSlow && (fjsx != 0.f || fjsy != 0.f || fjsz != 0.f)) {
+          atomicAddFixed(&a.force[3 * (size_t)a.stride + jatom], toFixedForce(fjsx));
+          atomicAddFixed(&a.force[4 * (size_t)a.stride + jatom], toFixedForce(fjsy));
+          atomicAddFixed(&a.force[5 * (size_t)a.stride + jatom], toFixedForce(fjsz));
         }
+        if (doEnergy) s_evg[wib][lane] += eV2.x + eV2.y;
+        if (kPrecise)
+          precisePass<doEnergy, doVirial, doSlow>(live, lane, s_ai[wib], s_aj[wib], s_pq[wib], T,
+                                                  c, lsum, npair);
       }
-      const int jatom = jstart + lane;
-      if (fjx != 0.f || fjy != 0.f || fjz != 0.f) {
-        atomicAddFixed(&a.force[0 * (size_t)a.stride + jatom], toFixedForce(fjx));
-        atomicAddFixed(&a.force[1 * (size_t)a.stride + jatom], toFixedForce(fjy));
-        atomicAddFixed(&a.force[2 * (size_t)a.stride + jatom], toFixedForce(fjz));
-      }
-      if (doSlow && (fjsx != 0.f || fjsy != 0.f || fjsz != 0.f)) {
-        atomicAddFixed(&a.force[3 * (size_t)a.stride + jatom], toFixedForce(fjsx));
-        atomicAddFixed(&a.force[4 * (size_t)a.stride + jatom], toFixedForce(fjsy));
-        atomicAddFixed(&a.force[5 * (size_t)a.stride + jatom], toFixedForce(fjsz));
-      }
-      if (doEnergy) {
-        if (doE64) {
-          eV += (double)eVt;
-        } else {
-          s_eg[wib][0][lane] += eVt;
-          s_eg[wib][1][lane] += eEt;
-          if (doSlow) s_eg[wib][2][lane] += eSt;
-        }
-      }
-      if (!doE64 && ((((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0) || jt == jtLast)) {
-        // end of a tile group: its energies and i forces into fixed point
+      if (((((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0) || jt == jtLast)) {
+        // end of a tile group: its LJ energy, i forces and precise-pass sums
+        // into fixed point
+        if (kPrecise) reduceGroup(lane, s_pq[wib], lsum, accQ);
         if (doEnergy) {
-#pragma unroll
-          for (int q = 0; q < 3; ++q) {
-            if (q == 2 && !doSlow) break;
-            s_eq[wib][q][lane] += toFixedEnergyF(s_eg[wib][q][lane]);
-            s_eg[wib][q][lane] = 0.f;
-          }
+          s_ev[wib][lane] += toFixedEnergyF(s_evg[wib][lane]);
+          s_evg[wib][lane] = 0.f;
         }
         s_fi[wib][0][lane] += (long long)toFixedForce(fix2.x + fix2.y);
         s_fi[wib][1][lane] += (long long)toFixedForce(fiy2.x + fiy2.y);
@@ -406,26 +536,15 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
 
     // i forces (fixed point)
     unsigned long long qx, qy, qz, sx = 0, sy = 0, sz = 0;
-    if (!doE64) {
-      qx = (unsigned long long)s_fi[wib][0][lane];
-      qy = (unsigned long long)s_fi[wib][1][lane];
-      qz = (unsigned long long)s_fi[wib][2][lane];
-      s_fi[wib][0][lane] = s_fi[wib][1][lane] = s_fi[wib][2][lane] = 0;
-      if (doSlow) {
-        sx = (unsigned long long)s_fi[wib][3][lane];
-        sy = (unsigned long long)s_fi[wib][4][lane];
-        sz = (unsigned long long)s_fi[wib][5][lane];
-        s_fi[wib][3][lane] = s_fi[wib][4][lane] = s_fi[wib][5][lane] = 0;
-      }
-    } else {
-      qx = toFixedForce(fix);
-      qy = toFixedForce(fiy);
-      qz = toFixedForce(fiz);
-      if (doSlow) {
-        sx = toFixedForce(fisx);
-        sy = toFixedForce(fisy);
-        sz = toFixedForce(fisz);
-      }
+    qx = (unsigned long long)s_fi[wib][0][lane];
+    qy = (unsigned long long)s_fi[wib][1][lane];
+    qz = (unsigned long long)s_fi[wib][2][lane];
+    s_fi[wib][0][lane] = s_fi[wib][1][lane] = s_fi[wib][2][lane] = 0;
+    if (doSlow) {
+      sx = (unsigned long long)s_fi[wib][3][lane];
+      sy = (unsigned long long)s_fi[wib][4][lane];
+      sz = (unsigned long long)s_fi[wib][5][lane];
+      s_fi[wib][3][lane] = s_fi[wib][4][lane] = s_fi[wib][5][lane] = 0;
     }
     if (qx | qy | qz) {
       atomicAddFixed(&a.force[0 * (size_t)a.stride + iatom], qx);
@@ -437,144 +556,117 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
       atomicAddFixed(&a.force[4 * (size_t)a.stride + iatom], sy);
       atomicAddFixed(&a.force[5 * (size_t)a.stride + iatom], sz);
     }
-    if (doVirial && doE64) {
-      // FP64 mode: the complete pair virial of this list, W = -sum g d (x) d
-      double tv[6], ts[6];
-#pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        tv[q] = warpSumD(wv[q]);
-        ts[q] = doSlow ? warpSumD(ws[q]) : 0.0;
-      }
-      if (lane < 18) {
-        const int q = symIndex(lane % 9);
-        double v = tv[0];
-#pragma unroll
-        for (int k = 1; k < 6; ++k)
-          if (k == q) v = (lane < 9) ? tv[k] : ts[k];
-        if (q == 0) v = (lane < 9) ? tv[0] : ts[0];
-        if (lane < 9 || doSlow) accVir += toFixedEnergy(v);
-      }
-    } else if (doVirial && !zeroShift) {
-      // the lattice-shift part of the virial, (sum_i F_i) (x) shift, is formed
-      // per compute by shiftVirialKernel from these exact integer sums
+    if (doVirial && !zeroShift) {
+      // the lattice-shift part of the fast virial, (sum_i F_i) (x) shift, is
+      // formed per compute by the finalize kernel from these exact integer sums
       const long long Fx = warpSumLL((long long)qx), Fy = warpSumLL((long long)qy),
                       Fz = warpSumLL((long long)qz);
-      long long Gx = 0, Gy = 0, Gz = 0;
-      if (doSlow) {
-        Gx = warpSumLL((long long)sx);
-        Gy = warpSumLL((long long)sy);
-        Gz = warpSumLL((long long)sz);
-      }
       long long* cf = a.compF + 6 * (size_t)tl.icompute;
       if (lane == 0) {
         if (Fx) atomicAddFixed(&cf[0], (unsigned long long)Fx);
         if (Fy) atomicAddFixed(&cf[1], (unsigned long long)Fy);
         if (Fz) atomicAddFixed(&cf[2], (unsigned long long)Fz);
-        if (doSlow) {
-          if (Gx) atomicAddFixed(&cf[3], (unsigned long long)Gx);
-          if (Gy) atomicAddFixed(&cf[4], (unsigned long long)Gy);
-          if (Gz) atomicAddFixed(&cf[5], (unsigned long long)Gz);
-        }
       }
     }
     if (doEnergy) {
-      long long sV, sE, sS = 0;
-      if (doE64) {
-        sV = toFixedEnergy(warpSumD(eV));
-        sE = toFixedEnergy(warpSumD(eE));
-        if (doSlow) sS = toFixedEnergy(warpSumD(eS));
-      } else {
-        sV = warpSumLL(s_eq[wib][0][lane]);
-        sE = warpSumLL(s_eq[wib][1][lane]);
-        if (doSlow) sS = warpSumLL(s_eq[wib][2][lane]);
-        s_eq[wib][0][lane] = s_eq[wib][1][lane] = s_eq[wib][2][lane] = 0;
-      }
-      if (lane == 0) {
-        if (doE64) {
-          accE0 += sV;
-          accE1 += sE;
-          accE2 += sS;
-        } else {
-          s_acc[wib][0] += sV;
-          s_acc[wib][1] += sE;
-          s_acc[wib][2] += sS;
-        }
-      }
+      const long long sV = warpSumLL(s_ev[wib][lane]);
+      s_ev[wib][lane] = 0;
+      if (lane == 0) s_evw[wib] += sV;
     }
   }  // lists
 
   // per-warp flush of the fixed-point accumulators (no block barrier, so a
   // warp that runs out of lists retires at once)
-  if (!doE64 && lane == 0) {
-    accE0 = s_acc[wib][0];
-    accE1 = s_acc[wib][1];
-    accE2 = s_acc[wib][2];
-  }
-  flushWarp<doEnergy, doVirial>(a.acc + (size_t)curRep * kAccCount, lane, accE0, accE1, accE2,
-                                accVir, npair);
+  if (lane == 0) accVdw = s_evw[wib];
+  flushWarp<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accVdw, accQ, npair);
 }
 
-template <bool E, bool V, bool S, bool D, bool B, int MINB>
-static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
-  const size_t shmem = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
-  auto k = forceKernel<E, V, S, D, B, MINB>;
-  static int cachedDim = -1, cachedBlocks = 0;
-  if (cachedDim != a.c.ljDim) {
-    if (shmem > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
-      if (e != cudaSuccess) return e;
-    }
-    int nb = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kForceThreads, shmem);
-    if (e != cudaSuccess) return e;
-    cachedBlocks = nb > 0 ? nb : 1;
-    cachedDim = a.c.ljDim;
+// Blocks per SM of one kernel instance on one device for one dynamic
+// shared-memory size, with the opt-in set on that device; looked up once per
+// (device, size) and kept per instance, under a lock, so handles on different
+// devices or threads neither share a stale entry nor race.
+constexpr int kMaxDevicesCached = 64;
+struct OccCache {
+  std::mutex mu;
+  size_t shmem[kMaxDevicesCached];
+  int blocks[kMaxDevicesCached];
+  OccCache() {
+    for (int d = 0; d < kMaxDevicesCached; ++d) shmem[d] = (size_t)-1, blocks[d] = 0;
   }
-  k<<<numSM * cachedBlocks, kForceThreads, shmem, st>>>(a);
+};
+
+// Dynamic shared memory of a force-kernel launch: the LJ table (single
+// system) and the transposed slow-term table when the precise pass reads it
+// from shared memory.
+size_t forceShmem(const ForceArgs& a, bool E, bool V, bool S, bool B) {
+  size_t bytes = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
+  if ((E || (V && S)) && S && a.slowTableShared)
+    bytes += sizeof(double) * kSlowTableDeg1 * (size_t)a.slowTableRows;
+  return bytes;
+}
+
+template <bool E, bool V, bool S, bool B, int MINB>
+static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
+  const size_t shmem = forceShmem(a, E, V, S, B);
+  auto k = forceKernel<E, V, S, B, MINB>;
+  static OccCache cache;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevicesCached) return cudaErrorInvalidDevice;
+  int blocks = 0;
+  {
+    std::lock_guard<std::mutex> lock(cache.mu);
+    if (cache.shmem[dev] != shmem) {
+      e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+      if (e != cudaSuccess) return e;
+      int nb = 0;
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kForceThreads, shmem);
+      if (e != cudaSuccess) return e;
+      cache.blocks[dev] = nb > 0 ? nb : 1;
+      cache.shmem[dev] = shmem;
+    }
+    blocks = cache.blocks[dev];
+  }
+  k<<<numSM * blocks, kForceThreads, shmem, st>>>(a);
   return cudaGetLastError();
 }
 
-template <bool E, bool V, bool S, bool D, bool B>
+template <bool E, bool V, bool S, bool B>
 static cudaError_t launchShape(const ForceArgs& a, int minBlocks, int numSM, cudaStream_t st) {
   switch (minBlocks) {
-    case 4: return launchT<E, V, S, D, B, 4>(a, numSM, st);
-    case 5: return launchT<E, V, S, D, B, 5>(a, numSM, st);
-    case 6: return launchT<E, V, S, D, B, 6>(a, numSM, st);
+    case 4: return launchT<E, V, S, B, 4>(a, numSM, st);
+    case 5: return launchT<E, V, S, B, 5>(a, numSM, st);
+    case 6: return launchT<E, V, S, B, 6>(a, numSM, st);
   }
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int numSM,
                         cudaStream_t st) {
-  const bool E = flags & NBK_ENERGY;
   const bool B = a.compRep != nullptr;
-  const int idx = (B ? 16 : 0) | (E ? 8 : 0) | ((flags & NBK_VIRIAL) ? 4 : 0) |
-                  ((flags & NBK_SLOW) ? 2 : 0) | ((E && (flags & NBK_ENERGY_FP64)) ? 1 : 0);
+  const int idx = (B ? 8 : 0) | ((flags & NBK_ENERGY) ? 4 : 0) | ((flags & NBK_VIRIAL) ? 2 : 0) |
+                  ((flags & NBK_SLOW) ? 1 : 0);
   switch (idx) {
-#define NBK_CASE(i, e, v, s, d, b) \
-  case i:                          \
-    return launchShape<e, v, s, d, b>(a, minBlocks, numSM, st);
-    NBK_CASE(0, false, false, false, false, false)
-    NBK_CASE(2, false, false, true, false, false)
-    NBK_CASE(4, false, true, false, false, false)
-    NBK_CASE(6, false, true, true, false, false)
-    NBK_CASE(8, true, false, false, false, false)
-    NBK_CASE(9, true, false, false, true, false)
-    NBK_CASE(10, true, false, true, false, false)
-    NBK_CASE(11, true, false, true, true, false)
-    NBK_CASE(12, true, true, false, false, false)
-    NBK_CASE(13, true, true, false, true, false)
-    NBK_CASE(14, true, true, true, false, false)
-    NBK_CASE(15, true, true, true, true, false)
-    // batched replicas (FP32 energy mode)
-    NBK_CASE(16, false, false, false, false, true)
-    NBK_CASE(18, false, false, true, false, true)
-    NBK_CASE(20, false, true, false, false, true)
-    NBK_CASE(22, false, true, true, false, true)
-    NBK_CASE(24, true, false, false, false, true)
-    NBK_CASE(26, true, false, true, false, true)
-    NBK_CASE(28, true, true, false, false, true)
-    NBK_CASE(30, true, true, true, false, true)
+#define NBK_CASE(i, e, v, s, b) \
+  case i:                       \
+    return launchShape<e, v, s, b>(a, minBlocks, numSM, st);
+    NBK_CASE(0, false, false, false, false)
+    NBK_CASE(1, false, false, true, false)
+    NBK_CASE(2, false, true, false, false)
+    NBK_CASE(3, false, true, true, false)
+    NBK_CASE(4, true, false, false, false)
+    NBK_CASE(5, true, false, true, false)
+    NBK_CASE(6, true, true, false, false)
+    NBK_CASE(7, true, true, true, false)
+    NBK_CASE(8, false, false, false, true)
+    NBK_CASE(9, false, false, true, true)
+    NBK_CASE(10, false, true, false, true)
+    NBK_CASE(11, false, true, true, true)
+    NBK_CASE(12, true, false, false, true)
+    NBK_CASE(13, true, false, true, true)
+    NBK_CASE(14, true, true, false, true)
+    NBK_CASE(15, true, true, true, true)
 #undef NBK_CASE
   }
   return cudaErrorInvalidValue;

@@ -116,56 +116,6 @@ __device__ __forceinline__ float erfcShared(const float x, const float ex) {
   return t * q * ex;
 }
 
-// FP32 pair math. f = (dE/dr)/r of LJ + fast electrostatics; fs = (dE/dr)/r
-// of the slow (PME real-space remainder) electrostatics. The caller applies
-// F_i += f (x_j - x_i), F_j -= f (x_j - x_i).
-//   LJ      E = (A r^-12 - B r^-6) S(r^2), S = 1 below rs, Hermite switch above
-//   fast    E = qq (1/r - (3 - r^2/rc^2)/(2 rc))
-//   slow    E = qq ((3 - r^2/rc^2)/(2 rc) + (erfc(beta r) - 1)/r)
-// (src/CudaComputeNonbondedInteractions.h:37-159 states the same forms.)
-template <bool doEnergy, bool doSlow>
-__device__ __forceinline__ void pairForce(const float r2, const float qq, const float2 ab,
-                                          const NbkConst& c, float& f, float& fs, float& eVdw,
-                                          float& eElec, float& eSlow) {
-  const float rinv = rsqrtf(r2);
-  const float rinv2 = rinv * rinv;
-  const float rinv6 = rinv2 * rinv2 * rinv2;
-  const float rinv3 = rinv * rinv2;
-  // switched LJ; t2 = max(r2, rs2) turns the switch off below rs exactly as
-  // the reference's branch does (S -> 1, dS -> 0 up to rounding)
-  const float ab6 = fmaf(ab.x, rinv6, -ab.y);           // A r^-6 - B
-  const float w = ab6 * rinv6;                           // A r^-12 - B r^-6
-  const float dw = fmaf(ab.x, rinv6, ab6) * (-6.0f * rinv2 * rinv6);  // (dw/dr)/r
-  float s = 1.0f, ds = 0.0f;
-  if (c.switching) {  // uniform over the grid
-    const float t2 = fmaxf(r2, c.rs2);
-    const float d = c.rc2 - t2;
-    s = d * d * fmaf(c.lj1, t2, c.lj0);
-    ds = d * fmaf(c.lj2, t2, c.lj3);
-  }
-  f = fmaf(w, ds, dw * s);
-  // fast electrostatics: qq (rc^-3 - r^-3)
-  f = fmaf(qq, c.rc3inv - rinv3, f);
-  float h = 0.0f;
-  if (doEnergy) {
-    eVdw = fmaf(w, s, eVdw);
-    h = fmaf(c.hB, r2, c.hA);
-    eElec = fmaf(qq, rinv - h, eElec);
-  }
-  if (doSlow) {
-    const float r = r2 * rinv;
-    const float x = c.beta * r;
-    const float ex = __expf(-x * x);
-    const float ec = erfcShared(x, ex);
-    // slow (dE/dr)/r = qq ((1 - erfc - 2b/sqrt(pi) r e^{-x^2}) r^-3 - rc^-3)
-    const float corr = fmaf(c.beta2Pi * r, ex, ec);
-    fs = qq * fmaf(1.0f - corr, rinv3, -c.rc3inv);
-    if (doEnergy) eSlow = fmaf(qq, fmaf(ec - 1.0f, rinv, h), eSlow);
-  } else {
-    fs = 0.0f;
-  }
-}
-
 // ---- two pairs at once with sm_100's packed FP32 instructions --------------
 // fma/mul/add .f32x2 issue two IEEE-rounded FP32 operations per instruction,
 // so every element below is rounded exactly as the scalar form would be;
@@ -197,17 +147,24 @@ __device__ __forceinline__ float rsqrtApprox(float x) {
   return y;
 }
 
-// pairForce for two pairs (x and y elements); nB = -B. An element with
-// qq = A = nB = 0 and r2 = cutoff^2 contributes exactly zero to f, fs and the
-// energies, which is how callers switch a pair off without a branch. The slow
-// term regroups the same quantities: with x = beta r, t = 1/(1 + p x) and
-// e = exp(-x^2) = 2^(gaussK r^2), erfc = t P(t) e and the force factor
-// erfc + (2 beta/sqrt(pi)) r e = (t P(t) + (2 beta/sqrt(pi)) r) e.
-template <bool doEnergy, bool doSlow>
+// FP32 pair math for two pairs (x and y elements); nB = -B. F, FS = (dE/dr)/r
+// of LJ + fast electrostatics and of the slow (PME real-space remainder)
+// electrostatics; the caller applies F_i += F (x_j - x_i), F_j -= F (x_j - x_i).
+//   LJ      E = (A r^-12 - B r^-6) S(r^2), S = 1 below rs, Hermite switch above
+//   fast    E = qq (1/r - (3 - r^2/rc^2)/(2 rc))
+//   slow    E = qq ((3 - r^2/rc^2)/(2 rc) + (erfc(beta r) - 1)/r)
+// (src/CudaComputeNonbondedInteractions.h:37-159 states the same forms.) Only
+// the LJ energy is summed here (doVdwEnergy): the electrostatic energies and
+// the slow virial are formed in FP64 by the force kernel's precise pass.
+// An element with qq = A = nB = 0 and r2 = cutoff^2 contributes exactly zero
+// to F, FS and the energy, which is how callers switch a pair off without a
+// branch. The slow term regroups the same quantities: with x = beta r,
+// t = 1/(1 + p x) and e = exp(-x^2) = 2^(gaussK r^2), erfc = t P(t) e and the
+// force factor erfc + (2 beta/sqrt(pi)) r e = (t P(t) + (2 beta/sqrt(pi)) r) e.
+template <bool doVdwEnergy, bool doSlow>
 __device__ __forceinline__ void pairForce2(const float2 r2, const float2 qq, const float2 A,
                                            const float2 nB, const NbkConst& c, float2& f,
-                                           float2& fs, float2& eVdw, float2& eElec,
-                                           float2& eSlow) {
+                                           float2& fs, float2& eVdw) {
   const float2 rinv = make_float2(rsqrtApprox(r2.x), rsqrtApprox(r2.y));
   const float2 rinv2 = mul2(rinv, rinv);
   const float2 rinv6 = mul2(mul2(rinv2, rinv2), rinv2);
@@ -223,12 +180,7 @@ __device__ __forceinline__ void pairForce2(const float2 r2, const float2 qq, con
   const float2 ds = mul2(d, fma2(f2(c.lj2), t2, f2(c.lj3)));
   f = fma2(w, ds, mul2(dw, s));
   f = fma2(qq, add2(f2(c.rc3inv), neg2(rinv3)), f);
-  float2 h = f2(0.0f);
-  if (doEnergy) {
-    eVdw = fma2(w, s, eVdw);
-    h = fma2(f2(c.hB), r2, f2(c.hA));
-    eElec = fma2(qq, add2(rinv, neg2(h)), eElec);
-  }
+  if (doVdwEnergy) eVdw = fma2(w, s, eVdw);
   if (doSlow) {
     const float2 r = mul2(r2, rinv);
     const float2 den = fma2(f2(c.pBeta), r, f2(1.0f));
@@ -243,50 +195,29 @@ __device__ __forceinline__ void pairForce2(const float2 r2, const float2 qq, con
     q = fma2(q, t, f2(kErfcC5));
     q = fma2(q, t, f2(kErfcC6));
     q = fma2(q, t, f2(kErfcC7));
-    const float2 tq = mul2(t, q);
-    const float2 corr = mul2(fma2(f2(c.beta2Pi), r, tq), ex);
+    const float2 corr = mul2(fma2(f2(c.beta2Pi), r, mul2(t, q)), ex);
     fs = mul2(qq, fma2(add2(f2(1.0f), neg2(corr)), rinv3, f2(-c.rc3inv)));
-    if (doEnergy) {
-      const float2 ec = mul2(tq, ex);
-      eSlow = fma2(qq, fma2(add2(ec, f2(-1.0f)), rinv, h), eSlow);
-    }
   } else {
     fs = f2(0.0f);
   }
 }
 
-// The same pair math in FP64 from FP64 geometry d = x_j - x_i (FP64 energy
-// mode): g, gs = (dE/dr)/r of LJ + fast and of slow electrostatics; adds the
-// electrostatic energies to eE, eS.
-template <bool doSlow>
-__device__ __forceinline__ void pairFP64(const double r2, const double qq, const double A,
-                                         const double B, const NbkConst64& k, double& g,
-                                         double& gs, double& eE, double& eS) {
-  const double ri = rsqrt(r2);
-  const double ri2 = ri * ri, ri6 = ri2 * ri2 * ri2, ri3 = ri * ri2;
-  const double ab6 = fma(A, ri6, -B);
-  const double w = ab6 * ri6;
-  const double dw = fma(A, ri6, ab6) * (-6.0 * ri2 * ri6);
-  double s = 1.0, ds = 0.0;
-  if (k.switching) {
-    const double t2 = fmax(r2, k.rs2);
-    const double d = k.rc2 - t2;
-    s = d * d * fma(k.lj1, t2, k.lj0);
-    ds = d * fma(k.lj2, t2, k.lj3);
-  }
-  g = fma(w, ds, dw * s) + qq * (k.rc3inv - ri3);
-  const double h = fma(k.hB, r2, k.hA);
-  eE = fma(qq, ri - h, eE);
-  if (doSlow) {
-    const double r = r2 * ri, x = k.beta * r;
-    const double ec = erfc(x), ex = exp(-x * x);
-    gs = qq * fma(1.0 - ec - k.beta2Pi * r * ex, ri3, -k.rc3inv);
-    eS = fma(qq, fma(ec - 1.0, ri, h), eS);
-  } else {
-    gs = 0.0;
-  }
-}
-
+// ---- the FP64 slow-term table ------------------------------------------------
+// The slow electrostatic energy per unit qq, phi_s(s) = h(s) - erf(beta sqrt(s))/sqrt(s)
+// with s = r^2 and h(s) = (3 - s/rc^2)/(2 rc), is an entire function of s (the
+// 1/r singularities of erfc(beta r)/r and of the fast part cancel), so a
+// piecewise polynomial in s represents it to FP64 rounding: with a step D (a
+// power of two, at most 2 A^2), row k holds the degree-6 Chebyshev
+// interpolant on s in [k D - D/2, k D + D/2] in the monomial basis of
+// w = s - k D (7 coefficients and a zero pad, 64 bytes). Its derivative gives
+// the slow force factor, (dE/dr)/r = 2 qq phi_s'(s), without the
+// rc^-3 - r^-3 cancellation of the FP32 form. Built on the host at handle
+// creation (buildSlowTable) from FP64 erf, with D chosen so that the fit is
+// within FP64 rounding.
+constexpr double kSlowTableStepMax = 2.0;  // A^2
+constexpr int kSlowTableDeg = 6;
+constexpr int kSlowTableDeg1 = kSlowTableDeg + 1;  // coefficients per row
+constexpr int kSlowTableRow = 8;        // doubles per row
 // Component k (0..8, row-major 3x3) of a symmetric tensor stored as
 // xx, xy, xz, yy, yz, zz.
 __device__ __forceinline__ int symIndex(int k) {
@@ -349,8 +280,11 @@ struct ForceArgs {
   long long* acc;              // [kAccCount]
   int* workCounter;            // next work item to hand out (zeroed before the launch)
   int splitLog2;               // force kernel: 2^splitLog2 work items per list
-  long long* compF;            // FP32 mode with virial: [numComputes][6] i-force sums per compute
-  NbkConst64 c64;              // FP64 energy/virial mode
+  long long* compF;            // virial: [numComputes][6] i-force sums per compute (0..2 used)
+  const double2* slowTable;    // [slowTableRows * kSlowTableRow / 2] phi_s rows (FP64)
+  int slowTableRows;
+  double slowStep, slowInvStep;  // table step D (a power of two) and 1/D
+  int slowTableShared;         // 1: the kernel copies the table into shared memory
   // replicas (batched evaluation; all NULL for a single system)
   const int* compRep;          // [numComputes] replica of each compute
   const float3* repLat;        // [3*numReplicas] lattice vectors a, b, c

@@ -4,10 +4,18 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "nbk_internal.cuh"
 
 namespace nbk {
+
+// Pair-math constants from the caller's parameters (nbk_consts.cu); shared by
+// the handle and by the allocation-free entry point.
+void makeConstants(const nbk_params& p, int ljDim, NbkConst& c, NbkConst64& k);
+// The FP64 slow-term table of the force kernel's precise pass; returns rows.
+int buildSlowTable(double beta, double cutoff, double pairlistdist, std::vector<double>& out,
+                   double* step);
 
 // minBlocks: 4, 5 or 6 CTAs per SM (the register cap); a.splitLog2 set by the caller.
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int numSM,
@@ -59,14 +67,15 @@ cudaError_t launchCorrections(const CorrArgs& a, unsigned flags, cudaStream_t st
 // from the exact integer i-force sums the force kernel leaves per compute.
 struct ShiftVirialArgs {
   int numComputes;
-  const long long* compF;                // [numComputes][6]
+  const long long* compF;                // [numComputes][6] (0..2: fast i-force sums)
   const nbk_compute_record* computes;
   float3 lata, latb, latc;
   const int* compRep;                    // batched replicas, else NULL
   const float3* repLat;
 };
 
-// shift: also folds the shift virial into the accumulators (FP32 virial mode).
+// With NBK_VIRIAL: the per-atom part of the fast virial, and with shift also
+// its lattice-shift part, into the accumulators.
 cudaError_t launchFinalizeForces(int n, const long long* force, int stride, const float4* xyzq,
                                  float4* outF, float4* outS, unsigned flags, long long* acc,
                                  int numSM, cudaStream_t st, const int* slotRep = nullptr,

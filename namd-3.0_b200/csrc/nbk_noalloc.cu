@@ -72,49 +72,6 @@ int scratchFor(int device, long long** out) {
   return NBK_OK;
 }
 
-void makeConsts(const nbk_params& p, int ljDim, NbkConst& c, NbkConst64& k) {
-  const double rc = p.cutoff, rc2 = rc * rc;
-  const bool sw = p.switchdist < p.cutoff;
-  const double rs2 = sw ? p.switchdist * p.switchdist : rc2;
-  const double c1 = sw ? 1.0 / ((rc2 - rs2) * (rc2 - rs2) * (rc2 - rs2)) : 0.0;
-  std::memset(&c, 0, sizeof(c));
-  c.cutoff2 = (float)rc * (float)rc;
-  c.plcutoff2 = (float)p.pairlistdist * (float)p.pairlistdist;
-  c.rc2 = (float)rc2;
-  c.rs2 = (float)rs2;
-  c.lj0 = (float)(c1 * (rc2 - 3.0 * rs2));
-  c.lj1 = (float)(2.0 * c1);
-  c.lj2 = (float)(-12.0 * c1);
-  c.lj3 = (float)(12.0 * c1 * rs2);
-  c.rc3inv = (float)(1.0 / (rc * rc2));
-  c.hA = (float)(1.5 / rc);
-  c.hB = (float)(-0.5 / (rc * rc2));
-  c.beta = (float)p.ewaldcof;
-  c.beta2Pi = (float)(2.0 * p.ewaldcof / std::sqrt(M_PI));
-  c.one14 = (float)(1.0 - p.scale14);
-  c.pBeta = (float)(kErfcP * p.ewaldcof);
-  c.gaussK = (float)(-p.ewaldcof * p.ewaldcof / std::log(2.0));
-  c.ljDim = ljDim;
-  c.switching = sw ? 1 : 0;
-  c.s0 = sw ? 0.0f : 1.0f;
-  c.hAd = 1.5 / rc;
-  c.hBd = -0.5 / (rc * rc2);
-  c.betad = p.ewaldcof;
-  k.rc2 = rc2;
-  k.rs2 = rs2;
-  k.lj0 = c1 * (rc2 - 3.0 * rs2);
-  k.lj1 = 2.0 * c1;
-  k.lj2 = -12.0 * c1;
-  k.lj3 = 12.0 * c1 * rs2;
-  k.rc3inv = 1.0 / (rc * rc2);
-  k.hA = 1.5 / rc;
-  k.hB = -0.5 / (rc * rc2);
-  k.beta = p.ewaldcof;
-  k.beta2Pi = 2.0 * p.ewaldcof / std::sqrt(M_PI);
-  k.one14 = 1.0 - p.scale14;
-  k.switching = sw ? 1 : 0;
-}
-
 }  // namespace
 
 extern "C" NBK_API const char* nbk_noalloc_last_error(void) { return g_noallocErr.c_str(); }
@@ -136,7 +93,10 @@ extern "C" NBK_API int nbk_exclusion_force_noalloc(
   if (atomStorageSize <= 0 || atomStorageSize > kNoAllocMaxSlots)
     return fail(NBK_ERR_ARG, "nbk_exclusion_force_noalloc: atomStorageSize must be in 1.." +
                                  std::to_string(kNoAllocMaxSlots) + " (the static scratch limit)");
-  if (numModified < 0 || numExcluded < 0 || numModified + numExcluded > kNoAllocMaxTuples)
+  // each count on its own, then the sum in 64 bits, so no overflow can pass
+  if (numModified < 0 || numExcluded < 0 || numModified > kNoAllocMaxTuples ||
+      numExcluded > kNoAllocMaxTuples ||
+      (long long)numModified + (long long)numExcluded > (long long)kNoAllocMaxTuples)
     return fail(NBK_ERR_ARG, "nbk_exclusion_force_noalloc: more than " +
                                  std::to_string(kNoAllocMaxTuples) +
                                  " tuples (the static scratch limit)");
@@ -188,7 +148,7 @@ extern "C" NBK_API int nbk_exclusion_force_noalloc(
   ca.lata = make_float3(lata.x, lata.y, lata.z);
   ca.latb = make_float3(latb.x, latb.y, latb.z);
   ca.latc = make_float3(latc.x, latc.y, latc.z);
-  makeConsts(*params, dim, ca.c, ca.c64);
+  makeConstants(*params, dim, ca.c, ca.c64);
   ca.force = force;
   ca.stride = n;
   ca.acc = acc;

@@ -359,6 +359,8 @@ def dev_lib() -> C.CDLL:
         lib.nbk_launch_count.argtypes = [vp]
         lib.nbk_get_pair_count.argtypes = [vp, C.POINTER(C.c_longlong), vp]
         lib.nbk_measure_fp32_peak.argtypes = [i, C.POINTER(C.c_double)]
+        lib.nbk_slow_table.argtypes = [C.c_double, C.c_double, C.c_double, vp, i,
+                                       C.POINTER(C.c_double)]
         lib.nbk_set_replicas.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp]
         lib.nbk_adjoint.argtypes = [vp, u, vp, vp, C.c_double, C.c_double, C.c_double, vp, vp, vp,
                                     vp, vp]
@@ -631,6 +633,22 @@ class Nonbonded:
                                         ja.ctypes.data, ex.ctypes.data, stream),
                 "nbk_export_tile_lists")
         return tl[:nl.value], ja[:nj.value], ex[:nj.value]
+
+
+def slow_table(ewaldcof: float, cutoff: float, pairlistdist: float):
+    """The FP64 slow-term table of the precise pass (nbk_slow_table): (rows,
+    step) where row k holds c0..c6 of phi_s(s) ~ sum c_n (s - k step)^n on
+    s in [k step - step/2, k step + step/2] (and a zero); host-only."""
+    L = dev_lib()
+    rows = L.nbk_slow_table(ewaldcof, cutoff, pairlistdist, None, 0, None)
+    if rows <= 0:
+        raise NbkError(f"nbk_slow_table failed ({rows})")
+    out = np.zeros((rows, 8))
+    step = C.c_double(0.0)
+    rc = L.nbk_slow_table(ewaldcof, cutoff, pairlistdist, out.ctypes.data, rows, C.byref(step))
+    if rc != rows:
+        raise NbkError(f"nbk_slow_table failed ({rc})")
+    return out, step.value
 
 
 def measure_fp32_peak(device: int = 0) -> float:

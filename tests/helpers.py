@@ -9,17 +9,8 @@ ALL = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
 
 # tolerances (relative to the FP64 oracle)
 FORCE_RMS_TOL = 1e-5      # RMS relative force error
-ENERGY_TOL = 1e-6         # relative error of each energy term (FP64 energy mode; LJ always)
+ENERGY_TOL = 1e-6         # relative error of each energy term
 VIRIAL_TOL = 1e-6         # Frobenius-relative virial error
-# FP32 energy mode: each electrostatic pair energy carries ~1e-7 relative FP32
-# error, so a total that cancels to 1/2e4 of the sum of |pair energies| (the
-# random-orientation water here) is resolved to ~1e-5 of itself.
-FP32_ELEC_ENERGY_TOL = 5e-5
-# FP32 energy mode: the virial is sum F_i (x) x_i over FP32 pair forces. Near
-# the cutoff the electrostatic split rc^-3 - r^-3 cancels, which leaves the
-# slow virial (small next to its terms) at about 1e-6 of itself; the FP64
-# energy/virial mode (NBK_ENERGY_FP64) holds VIRIAL_TOL with a wide margin.
-FP32_VIRIAL_TOL = 2e-6
 
 
 def water_box(seed=1, nwater=3000, box=44.8):

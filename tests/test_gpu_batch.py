@@ -5,7 +5,8 @@ import pytest
 
 import nbk
 import oracle
-from helpers import ALL, FORCE_RMS_TOL, PARAMS, mixed_box, real_slots, rms_rel
+from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, PARAMS, VIRIAL_TOL, compare, mixed_box,
+                     real_slots)
 
 pytestmark = pytest.mark.gpu
 
@@ -58,30 +59,38 @@ def test_batch_equals_single_handles(replicas, corr):
         assert counts[r] == cnt, r
 
 
-def test_batch_replica_against_oracle(replicas):
+@pytest.mark.parametrize("corr", [False, True])
+def test_batch_replicas_against_oracle(replicas, corr):
+    """Every replica of one batched evaluation against its own FP64 oracle:
+    forces, and energies and virials at 1e-6, on the pairlist step and on a
+    steady step."""
     import torch
     systems, many = replicas
+    flags = ALL | (nbk.NBK_CORRECTIONS if corr else 0)
     nb = nbk.Nonbonded(PARAMS, systems[0].lj_table())
     nb.setup(many)
     nb.set_replicas(many)
     X = torch.zeros((6, many.atomStorageSize), dtype=torch.int64, device="cuda")
     nb.build_tile_lists(many)
-    nb.force(many, ALL | nbk.NBK_PAIRLIST, xyzq=many.xyzq, d_fixed=X)
-    r = 3
-    p = nbk.Packed(systems[r])
-    Fo, So, ro = oracle.Oracle(p, PARAMS).forces(1)
     ss = many.replicaSlotStart
-    F = X[:3, ss[r]:ss[r + 1]].T.cpu().numpy() / nbk.FORCE_FIXED_SCALE
-    real = real_slots(p)
-    assert rms_rel(F[real], Fo[real]) <= FORCE_RMS_TOL
-    assert nb.pair_counts()[r] == ro["pairs"]
-
-
-def test_batch_rejects_fp64_energy(replicas):
-    systems, many = replicas
-    nb = nbk.Nonbonded(PARAMS, systems[0].lj_table())
-    nb.setup(many)
-    nb.set_replicas(many)
-    nb.build_tile_lists(many)
-    with pytest.raises(nbk.NbkError, match="not available with replicas"):
-        nb.force(many, ALL | nbk.NBK_PAIRLIST | nbk.NBK_ENERGY_FP64, xyzq=many.xyzq)
+    for step in (flags | nbk.NBK_PAIRLIST, flags):
+        nb.force(many, step, xyzq=many.xyzq, d_fixed=X)
+        ves = nb.virial_energy_batch()
+        counts = nb.pair_counts()
+        Xb = X.cpu().numpy()
+        for r, system in enumerate(systems):
+            p = nbk.Packed(system)
+            Fo, So, ro = oracle.Oracle(p, PARAMS).forces(3 if corr else 1)
+            real = real_slots(p)
+            F = Xb[:3, ss[r]:ss[r + 1]].T / nbk.FORCE_FIXED_SCALE
+            S = Xb[3:, ss[r]:ss[r + 1]].T / nbk.FORCE_FIXED_SCALE
+            res = dict(energyVdw=ves[r].energyVdw, energyElec=ves[r].energyElec,
+                       energySlow=ves[r].energySlow,
+                       virial=np.array(ves[r].virial).reshape(3, 3),
+                       virialSlow=np.array(ves[r].virialSlow).reshape(3, 3))
+            err = compare(F, S, res, Fo, So, ro, real)
+            assert err["force"] <= FORCE_RMS_TOL and err["slow"] <= FORCE_RMS_TOL, (r, err)
+            for k in ("energyVdw", "energyElec", "energySlow"):
+                assert err[k] <= ENERGY_TOL, (r, k, err)
+            assert err["virial"] <= VIRIAL_TOL and err["virialSlow"] <= VIRIAL_TOL, (r, err)
+            assert counts[r] == ro["pairs"], r

@@ -3,20 +3,13 @@
 The system: 25% seeded random-walk chains + TIP3P-like water at 0.1 atoms/A^3
 (a 220.1 A periodic cube), cutoff 12 / switch 10 / pairlist 13.5 A, 1-2/1-3
 exclusions, 1-4 pairs scaled 0.833, the exclusion corrections included.
-Forces use FP32 pair math folded into 64-bit fixed point; energies and virials
-are reported for the FP32 mode and the FP64 energy/virial mode. Force errors are
-measured against the FP64 oracle on a seeded 10,000-atom subset; energies and
-virials are whole-system quantities. The table is printed as one JSON line.
-
-At this size the electrostatic totals are tiny remainders of cancelling sums
-(E_elec is about 1e-6 of the sum of |pair energies|), so FP32 pair energies,
-each rounded to ~1e-7 of itself, cannot resolve them: in FP32 mode their error
-is judged against the sum of |pair energies| (the bound FP32 accumulation can
-promise), and the FP64 energy/virial mode is held to 1e-6 of the totals. The
-FP32-mode slow virial grows to about 3e-6 here: the fast/slow split of each
-pair force carries the factor r^-3 - rc^-3, whose direct FP32 difference
-cancels near the cutoff, and the slow virial is small next to its terms; it is
-held to 5e-6 in FP32 mode (the FP64 mode computes pair virials in FP64).
+Forces use FP32 pair math folded into 64-bit fixed point; the electrostatic
+energies and the slow virial are formed per pair in FP64 and the LJ energy and
+fast virial in FP32 (see nbk_nonbonded_force). Force errors are measured
+against the FP64 oracle on a seeded 10,000-atom subset; energies and virials
+are whole-system quantities, each held to 1e-6 of itself although the
+electrostatic totals are ~1e-6 of the sum of |pair energies| here. The table
+is printed as one JSON line.
 """
 import json
 
@@ -30,7 +23,6 @@ from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, PARAMS, VIRIAL_TOL, GpuRun,
 pytestmark = pytest.mark.gpu
 
 NATOMS, FRAC, SEED, SUBSET = 1066628, 0.25, 4, 10000
-LARGE_FP32_VIRIAL_TOL = 5e-6
 
 
 def test_large_system_error_table():
@@ -47,7 +39,7 @@ def test_large_system_error_table():
              "pairs_in_cutoff": int(ro["pairs"]),
              "energyElec_over_abs_sum": float(abs(ro["energyElec"]) / ro["absElec"])}
     extra = nbk.NBK_CORRECTIONS
-    for mode, fl in (("fp32", ALL | extra), ("fp64_energy", ALL | extra | nbk.NBK_ENERGY_FP64)):
+    for mode, fl in (("mixed_precision", ALL | extra),):
         for step, f in (("pairlist", fl | nbk.NBK_PAIRLIST), ("steady", fl)):
             F, S, res, _ = run.eval(f)
             e = {
@@ -66,11 +58,7 @@ def test_large_system_error_table():
             table[f"{mode}_{step}"] = {k: float(f"{v:.3e}") for k, v in e.items()}
             assert e["force_rms"] <= FORCE_RMS_TOL and e["slow_rms"] <= FORCE_RMS_TOL, (mode, e)
             assert e["energyVdw"] <= ENERGY_TOL, (mode, e)
-            vtol = VIRIAL_TOL if mode == "fp64_energy" else LARGE_FP32_VIRIAL_TOL
-            if mode == "fp64_energy":
-                assert e["energyElec"] <= ENERGY_TOL and e["energySlow"] <= ENERGY_TOL, (mode, e)
-            else:
-                assert e["energyElec_vs_abs"] <= 1e-7 and e["energySlow_vs_abs"] <= 1e-7, (mode, e)
-            assert e["virial"] <= vtol and e["virialSlow"] <= vtol, (mode, e)
+            assert e["energyElec"] <= ENERGY_TOL and e["energySlow"] <= ENERGY_TOL, (mode, e)
+            assert e["virial"] <= VIRIAL_TOL and e["virialSlow"] <= VIRIAL_TOL, (mode, e)
     assert run.nb.pair_count() == ro["pairs"]
     print("large-system error table " + json.dumps(table))

@@ -4,8 +4,7 @@ import pytest
 
 import nbk
 import oracle
-from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, FP32_ELEC_ENERGY_TOL, FP32_VIRIAL_TOL,
-                     PARAMS, VIRIAL_TOL,
+from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, PARAMS, VIRIAL_TOL,
                      GpuRun, compare, mixed_box, real_slots, rms_rel, water_box)
 
 pytestmark = pytest.mark.gpu
@@ -47,36 +46,32 @@ def test_pairset_mixed(mixed):
     _pairset_check(mixed[1], mixed[2])
 
 
-def _check_forces(system, corr, e64):
+def _check_forces(system, corr):
     s, p, o = system
     mode = 3 if corr else 1
-    extra = (nbk.NBK_CORRECTIONS if corr else 0) | (nbk.NBK_ENERGY_FP64 if e64 else 0)
+    extra = nbk.NBK_CORRECTIONS if corr else 0
     Fo, So, ro = o.forces(mode)
     run = GpuRun(p)
     run.build()
     real = real_slots(p)
-    etol = ENERGY_TOL if e64 else FP32_ELEC_ENERGY_TOL
-    vtol = VIRIAL_TOL if e64 else FP32_VIRIAL_TOL
     for flags in (ALL | nbk.NBK_PAIRLIST | extra, ALL | extra):
         F, S, res, _ = run.eval(flags)
         err = compare(F, S, res, Fo, So, ro, real)
         print(f"flags={flags} " + " ".join(f"{k}={v:.2e}" for k, v in err.items()))
         assert err["force"] <= FORCE_RMS_TOL and err["slow"] <= FORCE_RMS_TOL, err
         assert err["energyVdw"] <= ENERGY_TOL, err
-        assert err["energyElec"] <= etol and err["energySlow"] <= etol, err
-        assert err["virial"] <= vtol and err["virialSlow"] <= vtol, err
+        assert err["energyElec"] <= ENERGY_TOL and err["energySlow"] <= ENERGY_TOL, err
+        assert err["virial"] <= VIRIAL_TOL and err["virialSlow"] <= VIRIAL_TOL, err
 
 
 @pytest.mark.parametrize("corr", [False, True])
-@pytest.mark.parametrize("e64", [False, True])
-def test_forces_water(water, corr, e64):
-    _check_forces(water, corr, e64)
+def test_forces_water(water, corr):
+    _check_forces(water, corr)
 
 
 @pytest.mark.parametrize("corr", [False, True])
-@pytest.mark.parametrize("e64", [False, True])
-def test_forces_mixed(mixed, corr, e64):
-    _check_forces(mixed, corr, e64)
+def test_forces_mixed(mixed, corr):
+    _check_forces(mixed, corr)
 
 
 def test_pair_count(mixed):
@@ -120,7 +115,7 @@ def _sparse_case(s):
     keys, nex = o.pairs()
     run = GpuRun(p)
     run.build()
-    F, S, res, _ = run.eval(ALL | nbk.NBK_PAIRLIST | nbk.NBK_CORRECTIONS | nbk.NBK_ENERGY_FP64)
+    F, S, res, _ = run.eval(ALL | nbk.NBK_PAIRLIST | nbk.NBK_CORRECTIONS)
     tl, ja, ex = run.nb.export_tile_lists()
     mine = nbk.pairs_from_tile_lists(tl, ja, ex, p.atomStorageSize)
     assert np.array_equal(mine, keys)
@@ -133,7 +128,7 @@ def _sparse_case(s):
     for k in ("energyVdw", "energyElec", "energySlow"):
         assert abs(res[k] - ro[k]) <= 1e-6 * max(abs(ro[k]), 1e-12), (k, res[k], ro[k])
     # the steady step on the same (possibly empty) lists
-    F2, S2, res2, _ = run.eval(ALL | nbk.NBK_CORRECTIONS | nbk.NBK_ENERGY_FP64)
+    F2, S2, res2, _ = run.eval(ALL | nbk.NBK_CORRECTIONS)
     assert np.abs(F2[real] - Fo[real]).max() <= 1e-5 * scale
     return len(keys), int(p.patches[:, 0].astype(bool).sum()), len(p.patches)
 

@@ -1,0 +1,58 @@
+"""The FP64 slow-term table of the force kernel's precise pass (host-only):
+its polynomials against the slow pair energy written from scipy's FP64 erf,
+and their derivatives against the slow force factor."""
+import math
+
+import numpy as np
+import pytest
+from scipy.special import erf, erfc
+
+import nbk
+from helpers import PARAMS
+
+
+def _eval(T, step, s):
+    k = np.rint(s / step).astype(int)
+    w = s - step * k
+    c = T[k]
+    p = c[:, 6].copy()
+    dp = np.zeros_like(p)
+    for n in range(5, -1, -1):
+        dp = dp * w + p
+        p = p * w + c[:, n]
+    return p, dp
+
+
+# (ewaldcof, cutoff, pairlistdist): the benchmark's, and the Ewald coefficients
+# that PME tolerance 1e-6 gives for 10 and 8 A cutoffs
+@pytest.mark.parametrize("beta,cutoff,pl", [(PARAMS.ewaldcof, PARAMS.cutoff, PARAMS.pairlistdist),
+                                            (0.34, 10.0, 11.5), (0.43, 8.0, 9.5), (0.2, 14.0, 16.0)])
+def test_slow_table_matches_the_slow_term(beta, cutoff, pl):
+    T, step = nbk.slow_table(beta, cutoff, pl)
+    assert T.shape[1] == 8 and np.all(T[:, 7] == 0.0)
+    assert step <= 2.0 and math.log2(step) == round(math.log2(step))
+    # rows cover s up to pairlistdist^2 + 2
+    assert step * (T.shape[0] - 1) + step / 2 >= pl * pl + 2
+    s = np.linspace(1.0, pl * pl, 200001)
+    r = np.sqrt(s)
+    rc = cutoff
+    # E_slow per unit qq as the oracle writes it, h + (erfc(beta r) - 1)/r,
+    # and the force factor (dE/dr)/r per unit qq,
+    # -rc^-3 - (erfc - 1)/r^3 - (2 beta/sqrt(pi)) exp(-beta^2 r^2)/r^2
+    h = (3.0 - s / rc ** 2) / (2.0 * rc)
+    phi = h + (erfc(beta * r) - 1.0) / r
+    g = (-1.0 / rc ** 3 + erf(beta * r) / r ** 3
+         - 2.0 * beta / math.sqrt(math.pi) * np.exp(-beta * beta * s) / s)
+    p, dp = _eval(T, step, s)
+    assert np.abs(p - phi).max() <= 1e-14 * np.abs(phi).max()
+    # per pair, a slow virial term g r^2 is then off by < 2e-12 per unit qq
+    assert np.abs(2.0 * dp - g).max() <= 1e-11 * np.abs(g).max()
+
+
+def test_slow_table_rejects_bad_parameters():
+    L = nbk.dev_lib()
+    assert L.nbk_slow_table(0.26, -1.0, 13.5, None, 0, None) < 0
+    assert L.nbk_slow_table(0.26, 12.0, 11.0, None, 0, None) < 0
+    rows = L.nbk_slow_table(0.26, 12.0, 13.5, None, 0, None)
+    out = np.zeros((rows - 1, 8))
+    assert L.nbk_slow_table(0.26, 12.0, 13.5, out.ctypes.data, rows - 1, None) < 0
