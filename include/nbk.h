@@ -319,12 +319,12 @@ NBK_API const char* nbk_noalloc_last_error(void);
 
 /* No counterpart in the reference (its slow term comes from interpolated
  * texture tables, src/CudaNonbondedTables.C:158-303). The FP64 slow-term table
- * the force kernel's precise pass evaluates. With step D (*step; a power of
- * two, 2 A^2 or less, chosen so that the fit is within FP64 rounding), row k
- * (8 doubles) holds the degree-6 Chebyshev interpolant of
+ * the precise energy / virial kernel evaluates. With step D (*step; a power
+ * of two, 32 A^2 or less, chosen so that the fit is within FP64 rounding),
+ * row k (8 doubles) holds the degree-7 Chebyshev interpolant of
  * phi_s(s) = (3 - s/rc^2)/(2 rc) - erf(ewaldcof sqrt(s))/sqrt(s), s = r^2, on
- * s in [k D - D/2, k D + D/2], as coefficients c0..c6 of powers of (s - k D),
- * then a zero. The slow pair energy is qq phi_s(s), the slow force factor
+ * s in [k D - D/2, k D + D/2], as coefficients c0..c7 of powers of (s - k D).
+ * The slow pair energy is qq phi_s(s), the slow force factor
  * (dE/dr)/r = 2 qq phi_s'(s). Rows cover s up to pairlistdist^2 + 2.
  * Host-only (no GPU needed): returns the number of rows and, when out is not
  * NULL, writes them (maxRows must be at least that number); step may be NULL;

@@ -120,7 +120,8 @@ struct nbk_context {
   int maxListLen = 0;                // most j tiles a culled list can hold
   DBuf<int> jatom2;
   DBuf<nbk_tile_excl> excl2;
-  DBuf<int> counters;  // [0] lists kept, [1] j tiles kept, [2] force / [3] refine work counters
+  DBuf<int> counters;  // [0] lists kept, [1] j tiles kept, [2] force / [3] refine / [4] precise work counters
+  DBuf<unsigned> live;  // [j tiles][32] interacting-pair words of the last energy / virial evaluation
   bool built = false;     // tile lists built (sparse)
   bool refined = false;   // compacted lists valid
   float3 lata{}, latb{}, latc{};
@@ -215,8 +216,6 @@ ForceArgs refinedForceArgs(nbk_context* h, float cutoff2) {
   a.slowTableRows = h->slowTableRows;
   a.slowStep = h->slowStep;
   a.slowInvStep = 1.0 / h->slowStep;
-  // the precise pass reads the table from shared memory when it is small
-  a.slowTableShared = sizeof(double) * kSlowTableDeg1 * (size_t)h->slowTableRows <= 16 * 1024;
   if (h->nrep > 0) {
     a.compRep = h->compRep.p;
     a.repLat = h->repLat.p;
@@ -330,10 +329,10 @@ NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
   fin(h->slowTable.ensure(slow.size() / 2), "nbk_create: alloc");
   if (rc == NBK_OK) fin(cudaMemcpy(h->slowTable.p, slow.data(), sizeof(double) * slow.size(), cudaMemcpyHostToDevice), "nbk_create: copy");
   fin(h->acc.ensure(kAccCount), "nbk_create: alloc");
-  fin(h->counters.ensure(4), "nbk_create: alloc");
+  fin(h->counters.ensure(8), "nbk_create: alloc");
   fin(h->ve.ensure(1), "nbk_create: alloc");
   if (rc == NBK_OK) fin(cudaMemset(h->acc.p, 0, sizeof(long long) * kAccCount), "nbk_create: memset");
-  if (rc == NBK_OK) fin(cudaMemset(h->counters.p, 0, sizeof(int) * 4), "nbk_create: memset");
+  if (rc == NBK_OK) fin(cudaMemset(h->counters.p, 0, sizeof(int) * 8), "nbk_create: memset");
   if (rc != NBK_OK) {
     nbk_destroy(h);
     return rc;
@@ -370,6 +369,7 @@ NBK_API int nbk_destroy(nbk_handle h) {
   h->jatom2.release();
   h->excl2.release();
   h->counters.release();
+  h->live.release();
   h->force.release();
   h->acc.release();
   h->ve.release();
@@ -650,10 +650,20 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   a.lists = h->refinedLists();
   a.tileJatomStart = h->jatom2.p;
   a.tileExcls = h->excl2.p;
-  NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int), st), "nbk_nonbonded_force");
+  NBK_CUDA(cudaMemsetAsync(h->counters.p + 2, 0, sizeof(int) * 3, st), "nbk_nonbonded_force");
+  if (needsPrecise(flags)) {
+    NBK_CUDA(h->live.ensure((size_t)std::max(h->jcap, 1) * 32), "nbk_nonbonded_force");
+    a.liveOut = h->live.p;
+  }
   NBK_CUDA(launchForce(a, flags, h->tuneMinBlocks[key], h->numSM, st), "force kernel");
-  NBK_CUDA(timedEvent(h, false, st), "timing event");
   h->launches += 1;
+  if (needsPrecise(flags)) {
+    ForceArgs pa = a;
+    pa.workCounter = h->counters.p + 4;
+    NBK_CUDA(launchPrecise(pa, flags, h->numSM, st), "precise energy / virial kernel");
+    h->launches += 1;
+  }
+  NBK_CUDA(timedEvent(h, false, st), "timing event");
   if ((flags & NBK_CORRECTIONS) && (h->numMod || h->numExc)) {
     if (h->maxTupleSlot >= n)
       return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: a correction tuple names a slot beyond atomStorageSize");
@@ -1038,6 +1048,10 @@ NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* str
   const int n = h->atomStorageSize;
   const int accBlocks = h->nrep > 0 ? h->nrep : 1;
   ForceArgs a = refinedForceArgs(h, h->lastCutoff2);
+  if (needsPrecise(kflags)) {  // the timed force kernel stores live words
+    NBK_CUDA(h->live.ensure((size_t)std::max(h->jcap, 1) * 32), "nbk_autotune");
+    a.liveOut = h->live.p;
+  }
   const int maxSplitLog2 = 2;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   NBK_CUDA(cudaEventCreate(&e0), "nbk_autotune");

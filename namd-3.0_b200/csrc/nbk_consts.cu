@@ -60,13 +60,14 @@ void makeConstants(const nbk_params& p, int ljDim, NbkConst& c, NbkConst64& k) {
 namespace {
 
 // erf(beta sqrt(s)) / sqrt(s), an entire function of s: its power series
-// (2 beta/sqrt(pi)) sum_n (-beta^2 s)^n / (n! (2n + 1)) where beta^2 |s| is
-// small (also for s < 0), FP64 erf elsewhere.
+// (2 beta/sqrt(pi)) sum_n (-beta^2 s)^n / (n! (2n + 1)) for s < 0 (the first
+// row's fit reaches down to s = -D/2, where beta^2 |s| stays below ~10) and
+// where beta^2 s is small, FP64 erf elsewhere.
 double erfOverR(double beta, double s) {
-  if (std::fabs(beta * beta * s) < 0.5) {
+  if (s < 0.0 || beta * beta * s < 0.5) {
     const double x = -beta * beta * s;
     double term = 1.0, sum = 0.0;
-    for (int n = 0; n < 40; ++n) {
+    for (int n = 0; n < 80; ++n) {
       sum += term / (2 * n + 1);
       term *= x / (n + 1);
     }
@@ -83,9 +84,9 @@ static double slowPhi(double beta, double rc, double s) {
   return (3.0 - s / (rc * rc)) / (2.0 * rc) - erfOverR(beta, s);
 }
 
-// One table of the given power-of-two step: row k the degree-6 Chebyshev
-// interpolant (7 nodes) on s in [k step - step/2, k step + step/2] written in
-// powers of w = s - k step. Returns the largest deviation from phi_s at 8
+// One table of the given power-of-two step: row k the degree-7 Chebyshev
+// interpolant (8 nodes) on s in [k step - step/2, k step + step/2] written in
+// powers of w = s - k step. Returns the largest deviation from phi_s at 32
 // points per row between the nodes.
 static double fitSlowTable(double beta, double rc, double step, int rows, std::vector<double>& out) {
   const int deg = kSlowTableDeg, nn = kSlowTableDeg + 1;
@@ -112,8 +113,8 @@ static double fitSlowTable(double beta, double rc, double step, int rows, std::v
     }
     double scale = 1.0;
     for (int m = 0; m <= deg; ++m, scale /= half) row[m] = cu[m] * scale;
-    for (int q = 0; q < 8; ++q) {
-      const double w = half * (-1.0 + (q + 0.5) / 4.0);
+    for (int q = 0; q < 32; ++q) {
+      const double w = half * (-1.0 + (q + 0.5) / 16.0);
       double p = row[deg];
       for (int m = deg - 1; m >= 0; --m) p = p * w + row[m];
       worst = std::fmax(worst, std::fabs(p - slowPhi(beta, rc, centre + w)));
@@ -123,9 +124,9 @@ static double fitSlowTable(double beta, double rc, double step, int rows, std::v
 }
 
 // The slow-term table of the precise pass (layout in nbk_internal.cuh), over
-// s in [0, pairlistdist^2 + 2]. The step starts at 2 A^2 and is halved
-// (down to 1/16) until the fit is within 4e-15 of max |phi_s| (the
-// interpolation error of a row grows as beta^14 step^7). Returns the number
+// s in [0, pairlistdist^2 + 2]. The step starts at 32 A^2 and is halved
+// (down to 1/32 of that) until the fit is within 4e-15 of max |phi_s| (the
+// interpolation error of a row grows as (beta^2 step)^8). Returns the number
 // of rows; *stepOut receives the step.
 int buildSlowTable(double beta, double cutoff, double pairlistdist, std::vector<double>& out,
                    double* stepOut) {
@@ -136,7 +137,7 @@ int buildSlowTable(double beta, double cutoff, double pairlistdist, std::vector<
   for (;;) {
     rows = (int)std::ceil(smax / step + 0.5) + 1;
     const double err = fitSlowTable(beta, cutoff, step, rows, out);
-    if (err <= 4e-15 * scale || step <= kSlowTableStepMax / 16) break;
+    if (err <= 4e-15 * scale || step <= kSlowTableStepMax / 32) break;
     step *= 0.5;
   }
   if (stepOut) *stepOut = step;

@@ -1,7 +1,8 @@
-// Nonbonded force kernel of the B200 path.
+// Nonbonded force kernel of the B200 path, and the precise energy / virial
+// kernel that follows it on energy and virial evaluations.
 //
-// One warp owns one tile list (32 i atoms of one patch against the j tiles of
-// a compute's partner patch), as CudaComputeNonbondedKernel's
+// forceKernel: one warp owns one tile list (32 i atoms of one patch against
+// the j tiles of a compute's partner patch), as CudaComputeNonbondedKernel's
 // nonbondedForceKernel does (src/CudaComputeNonbondedKernel.cu:629-1644), but:
 //   - two pair steps per iteration run through sm_100's packed FP32
 //     instructions; j forces ride in registers and rotate with a shuffle, so
@@ -11,12 +12,15 @@
 //     refineKernel); a pairlist step refines, compacts, then runs this kernel;
 //   - per-tile FP32 partial forces are folded into 64-bit fixed point with
 //     integer atomics, so the summed forces do not depend on the order in
-//     which lists run;
-//   - on energy and virial evaluations the electrostatic energies and the
-//     slow virial are formed in FP64 by a precise pass over the tile's
-//     interacting pairs, compacted into a queue (see precisePass), and folded
-//     into fixed point per tile; the LJ energy is summed in FP32 per group of
-//     tiles and the fast virial comes from the fixed-point forces.
+//     which lists run; the LJ energy is summed in FP32 per group of tiles and
+//     folded the same way; the fast virial comes from the fixed-point forces;
+//   - on energy and virial evaluations it stores, per tile and lane, which of
+//     the lane's pairs interact (the live words).
+// preciseKernel: the electrostatic energies and the slow virial in FP64, from
+// the live words: per tile, the interacting pairs are compacted into a queue
+// and evaluated 32 at a time from FP64 geometry (see precisePass); its own
+// launch runs at higher occupancy than the register- and shared-memory-heavy
+// FP32 loop, which hides the FP64 dependency chains.
 #include "nbk_internal.cuh"
 #include "nbk_launch.h"
 
@@ -48,12 +52,17 @@ __device__ __forceinline__ void symSlots(int m, int& s0, int& s1) {
   s1 = m == 1 ? 3 : m == 2 ? 6 : m == 4 ? 7 : -1;
 }
 
-// Adds a warp's fixed-point accumulators to one replica's accumulator block:
-// lane 0 the LJ energy (accVdw) and, with the other lanes, the pair count;
-// lane q < kNumQ its precise-pass quantity (accQ).
+// Adds the force kernel's LJ energy (lane 0) to one replica's accumulators.
 template <bool doEnergy>
-__device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& accVdw,
-                                          long long& accQ, int& npair) {
+__device__ __forceinline__ void flushVdw(long long* acc, int lane, long long& accVdw) {
+  if (doEnergy && lane == 0 && accVdw != 0) atomicAddFixed(&acc[kAccEVdw], (unsigned long long)accVdw);
+  accVdw = 0;
+}
+
+// Adds the precise kernel's accumulators to one replica's block: lane
+// q < kNumQ its quantity q (accQ), and the warp's pair count.
+template <bool doEnergy>
+__device__ __forceinline__ void flushPrecise(long long* acc, int lane, long long& accQ, int& npair) {
   if (lane < kNumQ && accQ != 0) {
     if (lane == kQElec) {
       atomicAddFixed(&acc[kAccEElec], (unsigned long long)accQ);
@@ -67,13 +76,12 @@ __device__ __forceinline__ void flushWarp(long long* acc, int lane, long long& a
     }
   }
   if (doEnergy) {
-    if (lane == 0 && accVdw != 0) atomicAddFixed(&acc[kAccEVdw], (unsigned long long)accVdw);
     int s = npair;
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0 && s) atomicAddFixed(&acc[kAccNumPairs], (unsigned long long)s);
   }
-  accVdw = accQ = 0;
+  accQ = 0;
   npair = 0;
 }
 
@@ -87,25 +95,37 @@ struct LaneSums {
   double eE, eS, w0, w1, w2, w3, w4, w5;
 };
 
-// The slow-term table as the precise pass reads it: in shared memory,
-// coefficient n of row k at sh[n * rows + k] (a warp's lanes read one
-// coefficient of up to 32 rows per load, few bank conflicts), or else the
-// global row-major copy (8 doubles per row).
+// The slow-term table as the precise pass reads it. kCopies > 0: kCopies
+// interleaved copies in shared memory (s_slowTab), 16-byte pair n of row k of
+// copy c at s_slowTab[(k * P + n) * kCopies + c] with P = kSlowTableDeg1 / 2;
+// lane l reads copy l % kCopies, so with 8 copies the 8 lanes of a quarter
+// warp (one 16-byte bank group each) never conflict, whatever rows they read.
+// kCopies == 0: the global copy (kSlowTableRow doubles per row).
+extern __shared__ __align__(16) double2 s_slowTab[];
+
 struct SlowTable {
-  const double* sh;
   const double2* gl;
-  int rows;
   unsigned last;
   double step, invStep;
 };
 
+template <int kCopies>
+__device__ __forceinline__ double2 slowPair(const SlowTable& T, const unsigned k, const int n,
+                                            const int lane) {
+  if (kCopies > 0) {
+    return s_slowTab[(k * (kSlowTableDeg1 / 2) + n) * kCopies + (lane & (kCopies - 1))];
+  } else {
+    return __ldg(T.gl + (size_t)k * (kSlowTableRow / 2) + n);
+  }
+}
+
 // The FP64 terms of one interacting pair (qq = 0 contributes exact zeros):
-// the fast energy qq (1/r - h(s)) with 1/r from the FP32 approximation
+// the fast energy qq (1/r - h(s)) with 1/r from the FP64 approximation
 // refined by one Newton step, and from the slow-term table the slow energy
 // qq phi_s(s) and the slow virial -2 qq phi_s'(s) d (x) d.
-template <bool doEnergy, bool doVirial, bool doSlow>
+template <bool doEnergy, bool doVirial, bool doSlow, int kCopies>
 __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable& T,
-                                            const NbkConst& c, LaneSums& L) {
+                                            const NbkConst& c, const int lane, LaneSums& L) {
   const double s = fma(u.dz, u.dz, fma(u.dy, u.dy, u.dx * u.dx));
   double p = 0.0, dp = 0.0;
   if (doSlow) {
@@ -116,40 +136,26 @@ __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable&
     const double t = fmin(fma(s, T.invStep, magic), magic + (double)T.last);
     const unsigned k = (unsigned)__double2loint(t);
     const double wq = fma(-T.step, t - magic, s);
-    double c0, c1, c2, c3, c4, c5, c6;
-    if (T.sh) {
-      const double* col = T.sh + k;
-      c0 = col[0];
-      c1 = col[T.rows];
-      c2 = col[2 * T.rows];
-      c3 = col[3 * T.rows];
-      c4 = col[4 * T.rows];
-      c5 = col[5 * T.rows];
-      c6 = col[6 * T.rows];
-    } else {
-      const double2* row = T.gl + (size_t)k * (kSlowTableRow / 2);
-      const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2),
-                    c67 = __ldg(row + 3);
-      c0 = c01.x, c1 = c01.y, c2 = c23.x, c3 = c23.y, c4 = c45.x, c5 = c45.y, c6 = c67.x;
+    double cf[kSlowTableDeg1];
+#pragma unroll
+    for (int n = 0; n < kSlowTableDeg1; n += 2) {
+      const double2 v = slowPair<kCopies>(T, k, n / 2, lane);
+      cf[n] = v.x;
+      cf[n + 1] = v.y;
     }
     // Horner for p(w) and p'(w) together
-    p = c6;
-    dp = p;
-    p = fma(p, wq, c5);
-    dp = fma(dp, wq, p);
-    p = fma(p, wq, c4);
-    dp = fma(dp, wq, p);
-    p = fma(p, wq, c3);
-    dp = fma(dp, wq, p);
-    p = fma(p, wq, c2);
-    dp = fma(dp, wq, p);
-    p = fma(p, wq, c1);
-    dp = fma(dp, wq, p);
-    p = fma(p, wq, c0);
+    p = cf[kSlowTableDeg];
+    dp = 0.0;
+#pragma unroll
+    for (int n = kSlowTableDeg - 1; n >= 0; --n) {
+      dp = fma(dp, wq, p);
+      p = fma(p, wq, cf[n]);
+    }
   }
   if (doEnergy) {
-    // y0 has relative error below 2^-22; after the step, below 2^-43
-    const double y0 = (double)rsqrtApprox((float)s);
+    // y0 (rsqrt.approx.ftz.f64) has relative error below 2^-20; after one
+    // Newton step, below 2^-39
+    const double y0 = rsqrtApprox64(s);
     const double hs = 0.5 * s;
     const double y = fma(y0, fma(-hs * y0, y0, 0.5), y0);
     L.eE = fma(u.qq, y - fma(c.hBd, s, c.hAd), L.eE);
@@ -173,17 +179,17 @@ __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable&
 // warp compacts the tile's interacting pairs into a queue in shared memory
 // (entry = i | t << 5, lane-major order; at most 32 * 32 two-byte entries,
 // the 2 KB of pq) and processes them in FP64, two per lane per iteration
-// (entries e and e + 32: independent dependency chains; an entry past the
-// end gets d = (1, 0, 0) and qq = 0, which contributes exact zeros -- its
-// atoms may be one and the same atom, so their own distance, 0, would turn
-// the zero into a NaN), adding to the lane's group sums L. Every step is
-// warp-synchronous and the sums depend only on the tile group.
-template <bool doEnergy, bool doVirial, bool doSlow>
-__device__ __forceinline__ void precisePass(const unsigned live, const int lane,
-                                            const Atom64* __restrict__ ai,
-                                            const Atom64* __restrict__ aj, double* pq,
-                                            const SlowTable& T, const NbkConst& c, LaneSums& L,
-                                            int& npair) {
+// (entries e and e + 32: independent dependency chains). Lane l holds atom l
+// of the list's i tile (ai: the FP64 shifted position and charge) and of the
+// current j tile (aj, FP64), and a pair's atoms come by shuffles. An entry
+// past the end gets d = (1, 0, 0) and qq = 0, which contributes exact zeros
+// (its atoms may be one and the same atom, so their own distance, 0, would
+// turn the zero into a NaN). Every step is warp-synchronous and the sums
+// depend only on the tile group.
+template <bool doEnergy, bool doVirial, bool doSlow, int kCopies>
+__device__ __forceinline__ void precisePass(const unsigned live, const int lane, const double4 ai,
+                                            const double4 aj, double* pq, const SlowTable& T,
+                                            const NbkConst& c, LaneSums& L, int& npair) {
   const int n = __popc(live);
   if (doEnergy) npair += n;
   int incl = n;
@@ -196,28 +202,39 @@ __device__ __forceinline__ void precisePass(const unsigned live, const int lane,
   if (total == 0) return;  // warp-uniform
   unsigned short* q = reinterpret_cast<unsigned short*>(pq);
   int pos = incl - n;
-  for (unsigned w = live; w; w &= w - 1) q[pos++] = (unsigned short)(lane | ((__ffs(w) - 1) << 5));
+  // two set bits per iteration (the loop runs up to popc(live) / 2 times)
+  for (unsigned w = live; w;) {
+    const int t0 = __ffs(w) - 1;
+    w &= w - 1;
+    q[pos] = (unsigned short)(lane | (t0 << 5));
+    if (w) {
+      const int t1 = __ffs(w) - 1;
+      w &= w - 1;
+      q[pos + 1] = (unsigned short)(lane | (t1 << 5));
+    }
+    pos += 2;
+  }
   __syncwarp();
   for (int base = 0; base < total; base += 2 * kWarp) {  // warp-uniform
     PairTerms u[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int e = base + h * kWarp + lane;
-      if (e < total) {
-        const unsigned ent = q[e];
-        const int i = ent & 31, j = (i + (ent >> 5)) & 31;
-        const Atom64 A = ai[i], B = aj[j];
-        u[h].dx = B.x - A.x;
-        u[h].dy = B.y - A.y;
-        u[h].dz = B.z - A.z;
-        u[h].qq = A.q * B.q;
-      } else {
-        u[h].dx = 1.0;
-        u[h].dy = u[h].dz = u[h].qq = 0.0;
-      }
+      const bool valid = e < total;
+      const unsigned ent = valid ? q[e] : 0u;
+      const int i = ent & 31, j = (i + (ent >> 5)) & 31;
+      // every lane takes part in the shuffles
+      const double ax = __shfl_sync(0xffffffffu, ai.x, i), ay = __shfl_sync(0xffffffffu, ai.y, i),
+                   az = __shfl_sync(0xffffffffu, ai.z, i), aq = __shfl_sync(0xffffffffu, ai.w, i);
+      const double bx = __shfl_sync(0xffffffffu, aj.x, j), by = __shfl_sync(0xffffffffu, aj.y, j),
+                   bz = __shfl_sync(0xffffffffu, aj.z, j), bq = __shfl_sync(0xffffffffu, aj.w, j);
+      u[h].dx = valid ? bx - ax : 1.0;
+      u[h].dy = valid ? by - ay : 0.0;
+      u[h].dz = valid ? bz - az : 0.0;
+      u[h].qq = valid ? aq * bq : 0.0;
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) precisePair<doEnergy, doVirial, doSlow>(u[h], T, c, L);
+    for (int h = 0; h < 2; ++h) precisePair<doEnergy, doVirial, doSlow, kCopies>(u[h], T, c, lane, L);
   }
   __syncwarp();  // the queue is consumed before pq is written again
 }
@@ -254,17 +271,14 @@ __device__ __forceinline__ void reduceGroup(const int lane, double* pq, LaneSums
 // default); a.splitLog2: each list's j tiles are shared by 2^splitLog2
 // work items (warps), contiguous parts of equal tile count. Both are launch
 // choices of the autotuner; results do not depend on them (fixed-point sums
-// per tile group, precise-pass sums per tile).
+// per tile group).
 template <bool doEnergy, bool doVirial, bool doSlow, bool doBatch, int MINB>
 __global__ void __launch_bounds__(kForceThreads, MINB)
     forceKernel(const __grid_constant__ ForceArgs a) {
-  // the precise pass runs on energy evaluations and on virial evaluations
-  // with slow forces (it forms the slow virial)
-  constexpr bool kPrecise = doEnergy || (doVirial && doSlow);
-  constexpr int kPW = kPrecise ? kForceWarps : 1;
-  // dynamic: the LJ table [ljDim*ljDim] (single system), then, when it fits,
-  // the slow-term table in its transposed layout [7][rows] (precise pass)
-  extern __shared__ float2 s_lj[];
+  // the live words feed the precise kernel, which runs on energy evaluations
+  // and on virial evaluations with slow forces (it forms the slow virial)
+  constexpr bool kLive = doEnergy || (doVirial && doSlow);
+  extern __shared__ __align__(16) float2 s_lj[];  // [ljDim*ljDim] (single system)
   // the j tile as five rows (x, y, z, q, type bits) of 64 entries; entry m
   // holds the values of atoms m & 31 and (m & 31) ^ 16, so that the two
   // packed elements of iteration k, j = (lane + k) & 31 and j ^ 16, come from
@@ -281,43 +295,19 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
   __shared__ long long s_ev[kForceWarps][kWarp];
   __shared__ float s_evg[kForceWarps][kWarp];
   __shared__ long long s_evw[kForceWarps];
-  // precise pass: FP64 shifted i atoms of the list, FP64 j atoms of the tile,
-  // and the pair queue / lane partials (2 KB per warp)
-  __shared__ Atom64 s_ai[kPW][kWarp];
-  __shared__ Atom64 s_aj[kPW][kWarp];
-  __shared__ double s_pq[kPW][kNumQ * kWarp];
 
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const NbkConst& c = a.c;
   const int dim = c.ljDim;
-  const int ljWords = doBatch ? 0 : dim * dim;
-  SlowTable T;
-  T.rows = a.slowTableRows;
-  T.last = (unsigned)(a.slowTableRows - 1);
-  T.step = a.slowStep;
-  T.invStep = a.slowInvStep;
-  T.gl = a.slowTable;
-  T.sh = nullptr;
-  if (!doBatch)
-    for (int k = threadIdx.x; k < ljWords; k += blockDim.x) s_lj[k] = a.ljTable[k];
-  if (kPrecise && doSlow && a.slowTableShared) {
-    double* st = reinterpret_cast<double*>(s_lj + ljWords);
-    const double* g = reinterpret_cast<const double*>(a.slowTable);
-    for (int k = threadIdx.x; k < kSlowTableDeg1 * T.rows; k += blockDim.x) {
-      const int n = k / T.rows, r = k - n * T.rows;
-      st[k] = g[(size_t)r * kSlowTableRow + n];
-    }
-    T.sh = st;
+  if (!doBatch) {
+    for (int k = threadIdx.x; k < dim * dim; k += blockDim.x) s_lj[k] = a.ljTable[k];
+    __syncthreads();
   }
-  if (!doBatch || (kPrecise && doSlow && a.slowTableShared)) __syncthreads();
 
   const int numLists = a.numListsDev ? *a.numListsDev : a.numListsHost;
 
   long long accVdw = 0;  // lane 0: LJ energy to flush (batched replica change)
-  long long accQ = 0;    // lane q < kNumQ: precise-pass quantity q
-  LaneSums lsum{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // this lane's precise-pass group sums
-  int npair = 0;         // interacting pairs counted by this lane (energy evaluations)
 #pragma unroll
   for (int q = 0; q < 6; ++q) s_fi[wib][q][lane] = 0;
   s_ev[wib][lane] = 0;
@@ -350,7 +340,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           accVdw = s_evw[wib];
           s_evw[wib] = 0;
         }
-        flushWarp<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accVdw, accQ, npair);
+        flushVdw<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accVdw);
         curRep = rep;
       }
       la = a.repLat[3 * rep];
@@ -364,20 +354,6 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
 
     const int iatom = tl.iatomStart + lane;
     float4 xi = a.xyzq[iatom];
-    if (kPrecise) {
-      // FP64 shifted i atom: the shift formed in FP64 from the FP32 offsets
-      // and lattice (the exact lattice translation), without the FP32
-      // rounding of sh
-      const double sx = (double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x;
-      const double sy = (double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y;
-      const double sz = (double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z;
-      Atom64 ai;
-      ai.x = (double)xi.x + sx;
-      ai.y = (double)xi.y + sy;
-      ai.z = (double)xi.z + sz;
-      ai.q = (double)xi.w;
-      s_ai[wib][lane] = ai;
-    }
     xi.x = __fadd_rn(xi.x, sh.x);
     xi.y = __fadd_rn(xi.y, sh.y);
     xi.z = __fadd_rn(xi.z, sh.z);
@@ -391,6 +367,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
       const int jstart = a.tileJatomStart[jt];
       const unsigned mask = a.tileExcls[jt].excl[lane];
       const unsigned stepMask = __reduce_or_sync(0xffffffffu, mask);
+      unsigned live = 0;  // interacting pairs of this lane, TileExcl bit order
       if (stepMask != 0) {
         const float4 xj = a.xyzq[jstart + lane];
         const float tyj = __int_as_float(a.vdwTypes[jstart + lane]);
@@ -406,14 +383,6 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
         s_jt[wib][2][lane] = s_jt[wib][2][lane + kWarp] = ez;
         s_jt[wib][3][lane] = s_jt[wib][3][lane + kWarp] = eq;
         s_jt[wib][4][lane] = s_jt[wib][4][lane + kWarp] = et;
-        if (kPrecise) {
-          Atom64 aj;
-          aj.x = (double)xj.x;
-          aj.y = (double)xj.y;
-          aj.z = (double)xj.z;
-          aj.q = (double)xj.w;
-          s_aj[wib][lane] = aj;
-        }
         __syncwarp();
 
         // Iteration k takes steps k and k+16 together through the packed
@@ -426,7 +395,6 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
         float2 eV2 = f2(0.f);
         const float2 nXi = f2(-xi.x), nYi = f2(-xi.y), nZi = f2(-xi.z);
         int kLast = 0;
-        unsigned live = 0;   // precise pass: interacting pairs, TileExcl bit order
         unsigned mk = mask;  // bit k of the mask moved to bit 0 (and k+16 to 16)
 #pragma unroll 2
         for (int k = 0; k < 16; ++k, mk >>= 1) {
@@ -441,7 +409,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
           const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
           if (!__any_sync(0xffffffffu, aA || aB)) continue;
-          if (kPrecise) live |= ((aA ? 1u : 0u) | (aB ? 0x10000u : 0u)) << k;
+          if (kLive) live |= ((aA ? 1u : 0u) | (aB ? 0x10000u : 0u)) << k;
           const float2 TY = pA[256];
           const int tyA = __float_as_int(TY.x), tyB = __float_as_int(TY.y);
           const float2 abA = doBatch ? __ldg(&ljRow[ti + tyA]) : s_lj[ti + tyA];
@@ -508,14 +476,10 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           atomicAddFixed(&a.force[5 * (size_t)a.stride + jatom], toFixedForce(fjsz));
         }
         if (doEnergy) s_evg[wib][lane] += eV2.x + eV2.y;
-        if (kPrecise)
-          precisePass<doEnergy, doVirial, doSlow>(live, lane, s_ai[wib], s_aj[wib], s_pq[wib], T,
-                                                  c, lsum, npair);
       }
+      if (kLive) a.liveOut[(size_t)jt * kWarp + lane] = live;
       if (((((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0) || jt == jtLast)) {
-        // end of a tile group: its LJ energy, i forces and precise-pass sums
-        // into fixed point
-        if (kPrecise) reduceGroup(lane, s_pq[wib], lsum, accQ);
+        // end of a tile group: its LJ energy and i forces into fixed point
         if (doEnergy) {
           s_ev[wib][lane] += toFixedEnergyF(s_evg[wib][lane]);
           s_evg[wib][lane] = 0.f;
@@ -575,10 +539,107 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     }
   }  // lists
 
-  // per-warp flush of the fixed-point accumulators (no block barrier, so a
-  // warp that runs out of lists retires at once)
+  // per-warp flush of the LJ energy (no block barrier, so a warp that runs
+  // out of lists retires at once)
   if (lane == 0) accVdw = s_evw[wib];
-  flushWarp<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accVdw, accQ, npair);
+  flushVdw<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accVdw);
+}
+
+// The precise kernel: one warp per refined tile list (handed out by a global
+// counter in the force kernel's order, longest first). Per list the FP64
+// shifted i atoms go to shared memory (the shift formed in FP64 from the FP32
+// offsets and lattice: the exact lattice translation, without the FP32
+// rounding of the force kernel's shift); per tile with interacting pairs the
+// j atoms (FP32) and the precise pass; per group of kFoldTiles tiles (counted
+// from the list start, as the force kernel's) the lanes' sums go into fixed
+// point. Results do not depend on the order in which lists run.
+constexpr int kPreciseWarps = 8;
+constexpr int kPreciseThreads = kPreciseWarps * kWarp;
+
+template <bool doEnergy, bool doVirial, bool doSlow, bool doBatch, int kCopies>
+__global__ void __launch_bounds__(kPreciseThreads, 3)
+    preciseKernel(const __grid_constant__ ForceArgs a) {
+  __shared__ double s_pq[kPreciseWarps][kNumQ * kWarp];
+  const int lane = threadIdx.x & 31;
+  const int wib = threadIdx.x >> 5;
+  SlowTable T;
+  T.last = (unsigned)(a.slowTableRows - 1);
+  T.step = a.slowStep;
+  T.invStep = a.slowInvStep;
+  T.gl = a.slowTable;
+  if (doSlow && kCopies > 0) {
+    constexpr int P = kSlowTableDeg1 / 2;
+    for (int k = threadIdx.x; k < P * a.slowTableRows * kCopies; k += blockDim.x) {
+      const int pair = k / (kCopies > 0 ? kCopies : 1);  // row * P + n
+      s_slowTab[k] = a.slowTable[(size_t)(pair / P) * (kSlowTableRow / 2) + pair % P];
+    }
+    __syncthreads();
+  }
+  const int numLists = a.numListsDev ? *a.numListsDev : a.numListsHost;
+  long long accQ = 0;  // lane q < kNumQ: quantity q
+  int npair = 0;       // interacting pairs counted by this lane (energy evaluations)
+  LaneSums lsum{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  int curRep = 0;
+  for (;;) {
+    int L = 0;
+    if (lane == 0) L = atomicAdd(a.workCounter, 1);
+    L = __shfl_sync(0xffffffffu, L, 0);
+    if (L >= numLists) break;
+    const nbk_tile_list tl = a.lists[L];
+    if (tl.jtileEnd < tl.jtileStart) continue;  // empty (warp-uniform)
+    float3 la = a.lata, lb = a.latb, lc = a.latc;
+    if (doBatch) {
+      const int rep = __ldg(&a.compRep[tl.icompute]);
+      if (rep != curRep) {
+        flushPrecise<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accQ, npair);
+        curRep = rep;
+      }
+      la = a.repLat[3 * rep];
+      lb = a.repLat[3 * rep + 1];
+      lc = a.repLat[3 * rep + 2];
+    }
+    // this lane's i atom, shifted in FP64 by the shift formed in FP64 from the
+    // FP32 offsets and lattice (the exact lattice translation, without the
+    // FP32 rounding of the force kernel's shift)
+    const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
+    double4 ai;
+    {
+      const float4 xi = a.xyzq[tl.iatomStart + lane];
+      ai.x = (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x);
+      ai.y = (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y);
+      ai.z = (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z);
+      ai.w = (double)xi.w;
+    }
+    // the next tile's live word and j atom are loaded while the current tile
+    // is processed; the j-tile starts come 32 at a time (lane t holds tile
+    // jt0 + t) and are handed out by a shuffle
+    int jsBlock = 0;
+    unsigned liveNext = 0;
+    float4 xjNext = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int jt = tl.jtileStart; jt <= tl.jtileEnd; ++jt) {
+      const int t = (jt - tl.jtileStart) & 31;
+      if (t == 0) {
+        const int jtl = jt + lane;
+        jsBlock = jtl <= tl.jtileEnd ? a.tileJatomStart[jtl] : 0;
+        liveNext = a.liveOut[(size_t)jt * kWarp + lane];
+        xjNext = a.xyzq[__shfl_sync(0xffffffffu, jsBlock, 0) + lane];
+      }
+      const unsigned live = liveNext;
+      const float4 xj = xjNext;
+      if (jt < tl.jtileEnd && t < 31) {
+        liveNext = a.liveOut[(size_t)(jt + 1) * kWarp + lane];
+        xjNext = a.xyzq[__shfl_sync(0xffffffffu, jsBlock, t + 1) + lane];
+      }
+      if (__any_sync(0xffffffffu, live != 0u)) {
+        const double4 aj = make_double4((double)xj.x, (double)xj.y, (double)xj.z, (double)xj.w);
+        precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, ai, aj, s_pq[wib], T, a.c,
+                                                         lsum, npair);
+      }
+      if (((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0 || jt == tl.jtileEnd)
+        reduceGroup(lane, s_pq[wib], lsum, accQ);
+    }
+  }
+  flushPrecise<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accQ, npair);
 }
 
 // Blocks per SM of one kernel instance on one device for one dynamic
@@ -595,21 +656,9 @@ struct OccCache {
   }
 };
 
-// Dynamic shared memory of a force-kernel launch: the LJ table (single
-// system) and the transposed slow-term table when the precise pass reads it
-// from shared memory.
-size_t forceShmem(const ForceArgs& a, bool E, bool V, bool S, bool B) {
-  size_t bytes = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
-  if ((E || (V && S)) && S && a.slowTableShared)
-    bytes += sizeof(double) * kSlowTableDeg1 * (size_t)a.slowTableRows;
-  return bytes;
-}
-
-template <bool E, bool V, bool S, bool B, int MINB>
-static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
-  const size_t shmem = forceShmem(a, E, V, S, B);
-  auto k = forceKernel<E, V, S, B, MINB>;
-  static OccCache cache;
+template <typename K>
+static cudaError_t launchPersistent(K kernel, OccCache& cache, int threads, size_t shmem,
+                                    int numSM, cudaStream_t st, const ForceArgs& a) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -618,18 +667,26 @@ static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
   {
     std::lock_guard<std::mutex> lock(cache.mu);
     if (cache.shmem[dev] != shmem) {
-      e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shmem);
       if (e != cudaSuccess) return e;
       int nb = 0;
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kForceThreads, shmem);
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, shmem);
       if (e != cudaSuccess) return e;
       cache.blocks[dev] = nb > 0 ? nb : 1;
       cache.shmem[dev] = shmem;
     }
     blocks = cache.blocks[dev];
   }
-  k<<<numSM * blocks, kForceThreads, shmem, st>>>(a);
+  kernel<<<numSM * blocks, threads, shmem, st>>>(a);
   return cudaGetLastError();
+}
+
+template <bool E, bool V, bool S, bool B, int MINB>
+static cudaError_t launchT(const ForceArgs& a, int numSM, cudaStream_t st) {
+  static OccCache cache;
+  const size_t shmem = B ? 0 : sizeof(float2) * (size_t)a.c.ljDim * a.c.ljDim;
+  return launchPersistent(forceKernel<E, V, S, B, MINB>, cache, kForceThreads, shmem, numSM, st,
+                          a);
 }
 
 template <bool E, bool V, bool S, bool B>
@@ -662,6 +719,52 @@ cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int n
     NBK_CASE(8, false, false, false, true)
     NBK_CASE(9, false, false, true, true)
     NBK_CASE(10, false, true, false, true)
+    NBK_CASE(11, false, true, true, true)
+    NBK_CASE(12, true, false, false, true)
+    NBK_CASE(13, true, false, true, true)
+    NBK_CASE(14, true, true, false, true)
+    NBK_CASE(15, true, true, true, true)
+#undef NBK_CASE
+  }
+  return cudaErrorInvalidValue;
+}
+
+bool needsPrecise(unsigned flags) {
+  return (flags & NBK_ENERGY) || ((flags & NBK_VIRIAL) && (flags & NBK_SLOW));
+}
+
+template <bool E, bool V, bool S, bool B, int C>
+static cudaError_t launchPC(const ForceArgs& a, int numSM, cudaStream_t st) {
+  static OccCache cache;
+  const size_t shmem = (S && C > 0) ? sizeof(double) * kSlowTableDeg1 * (size_t)a.slowTableRows * C
+                                    : 0;
+  return launchPersistent(preciseKernel<E, V, S, B, C>, cache, kPreciseThreads, shmem, numSM, st,
+                          a);
+}
+
+// the table in shared memory with 8 interleaved copies when they fit in 32 KB
+// (64 rows), else read from global memory
+template <bool E, bool V, bool S, bool B>
+static cudaError_t launchP(const ForceArgs& a, int numSM, cudaStream_t st) {
+  if (sizeof(double) * kSlowTableDeg1 * (size_t)a.slowTableRows * 8 <= 32 * 1024)
+    return launchPC<E, V, S, B, 8>(a, numSM, st);
+  return launchPC<E, V, S, B, 0>(a, numSM, st);
+}
+
+cudaError_t launchPrecise(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st) {
+  if (!needsPrecise(flags)) return cudaSuccess;
+  const bool B = a.compRep != nullptr;
+  const int idx = (B ? 8 : 0) | ((flags & NBK_ENERGY) ? 4 : 0) | ((flags & NBK_VIRIAL) ? 2 : 0) |
+                  ((flags & NBK_SLOW) ? 1 : 0);
+  switch (idx) {
+#define NBK_CASE(i, e, v, s, b) \
+  case i:                       \
+    return launchP<e, v, s, b>(a, numSM, st);
+    NBK_CASE(3, false, true, true, false)
+    NBK_CASE(4, true, false, false, false)
+    NBK_CASE(5, true, false, true, false)
+    NBK_CASE(6, true, true, false, false)
+    NBK_CASE(7, true, true, true, false)
     NBK_CASE(11, false, true, true, true)
     NBK_CASE(12, true, false, false, true)
     NBK_CASE(13, true, false, true, true)

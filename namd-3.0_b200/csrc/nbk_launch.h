@@ -20,6 +20,11 @@ int buildSlowTable(double beta, double cutoff, double pairlistdist, std::vector<
 // minBlocks: 4, 5 or 6 CTAs per SM (the register cap); a.splitLog2 set by the caller.
 cudaError_t launchForce(const ForceArgs& a, unsigned flags, int minBlocks, int numSM,
                         cudaStream_t st);
+// The precise energy / virial kernel after the force kernel (same lists, the
+// force kernel's live words, its own work counter a.workCounter); no-op when
+// flags need neither energies nor the slow virial.
+bool needsPrecise(unsigned flags);
+cudaError_t launchPrecise(const ForceArgs& a, unsigned flags, int numSM, cudaStream_t st);
 // Pairlist refinement of the culled lists a.lists[0, a.numListsHost): writes
 // a.tileExcls, a.jtileActive, a.listActive and the excluded-pair counts.
 cudaError_t launchRefine(const ForceArgs& a, int numSM, cudaStream_t st);

@@ -637,8 +637,9 @@ class Nonbonded:
 
 def slow_table(ewaldcof: float, cutoff: float, pairlistdist: float):
     """The FP64 slow-term table of the precise pass (nbk_slow_table): (rows,
-    step) where row k holds c0..c6 of phi_s(s) ~ sum c_n (s - k step)^n on
-    s in [k step - step/2, k step + step/2] (and a zero); host-only."""
+    step) where row k (8 doubles) holds c0..c7 of
+    phi_s(s) ~ sum c_n (s - k step)^n on s in [k step - step/2, k step + step/2];
+    host-only."""
     L = dev_lib()
     rows = L.nbk_slow_table(ewaldcof, cutoff, pairlistdist, None, 0, None)
     if rows <= 0:
