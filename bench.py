@@ -34,6 +34,11 @@ sys.path.insert(0, os.path.join(ROOT, "namd-3.0_b200"))
 METRIC = ("nonbonded pairs/s at 92k atoms (force err≤1e-5) vs plain GPU path & host CPU")
 UNIT = "pairs/s"
 FLOPS_PER_PAIR = 90          # algorithmic FP32 flops per interacting pair (FMA = 2)
+# algorithmic FP64 flops per interacting pair of the precise energy / virial
+# kernel (FMA = 2): d 3, r^2 5, qq 1, 1/r Newton step 6, h and fast energy 5,
+# slow-term polynomial and its derivative 26, slow energy 2, force factor 2,
+# slow virial 15
+FP64_FLOPS_PER_PAIR = 65
 NATOMS, BOX, FRAC = 92224, (108.0, 108.0, 78.0), 0.3
 NFRAMES, REBUILD, SIGMA = 100, 10, 0.02
 WORKLOAD = ("mixed-92224: 92,224 atoms (30% random-walk chains + TIP3P-like water), "
@@ -354,6 +359,114 @@ def _factors(k):
     return f
 
 
+class _DeviceArray:
+    """A device buffer (address, shape) seen by torch.as_tensor."""
+
+    def __init__(self, ptr, shape):
+        self.__cuda_array_interface__ = {"shape": shape, "typestr": "<f4",
+                                         "data": (int(ptr), False), "version": 3}
+
+
+def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, value, flush):
+    """The reference's plain GPU path (its own tile-list and nonbonded kernels,
+    built from the reference tree into oracle/_ref; texture-table mode, its
+    choice whenever slow forces are on) on the same trajectory and protocol as
+    the timed region: force + energy + virial + slow every step, lists rebuilt
+    every REBUILD steps. Steady steps copy the frame on the device into the
+    reference's position buffer; pairlist steps hand it the page-locked host
+    frame, as its tile-list build takes positions from the host. The same
+    GPU-counted pairs per frame give its pairs/s. None when the harness is not
+    built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refgpu
+    if not refgpu.available():
+        return None
+    import torch
+    import nbk
+    dev = torch.device("cuda", local_rank)
+    n = packed.atomStorageSize
+    ref = refgpu.RefGpu(nbk.NonbondedParams(), sys_.lj_table(), do_table=1, device=local_rank)
+    ref.setup(packed)
+    rs = torch.cuda.ExternalStream(ref.stream_ptr)
+    state = {}
+
+    def step(k):
+        f = k % NFRAMES
+        if k % REBUILD == 0:
+            ref.eval(1, 1, 1, 1, pin[f].numpy())
+            ptr = refgpu.lib().refgpu_device_xyzq(ref._h)
+            if state.get("ptr") != ptr:
+                state["ptr"] = ptr
+                state["view"] = torch.as_tensor(_DeviceArray(ptr, (n, 4)), device=dev)
+        else:
+            with torch.cuda.stream(rs):
+                state["view"].copy_(frames[f])
+            ref.eval(0, 1, 1, 1, None)
+
+    for k in range(max(args.warmup, 3)):
+        step(k)
+    ref.sync()
+    ksteps = min(args.steps, 500)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(ksteps)]
+    for k in range(ksteps):
+        with torch.cuda.stream(rs):
+            flush.zero_()
+        ev[k][0].record(rs)
+        step(k)
+        ev[k][1].record(rs)
+    ref.sync()
+    ms = np.array([a.elapsed_time(b) for a, b in ev])
+    pairs = int(sum(pairs_of[k % NFRAMES] for k in range(ksteps)))
+    v = pairs / (ms.sum() * 1e-3)
+    out = {"value": v, "unit": UNIT, "steps": ksteps, "ms_per_step": float(ms.mean()),
+           "steady_ms": float(np.mean([ms[k] for k in range(ksteps) if k % REBUILD])),
+           "pairlist_ms": float(np.mean([ms[k] for k in range(ksteps) if k % REBUILD == 0])),
+           "mode": "reference CudaTileListKernel + CudaComputeNonbondedKernel, texture tables",
+           "product_over_reference": value / v}
+    del ref
+    return out
+
+
+def frame0_errors(nb, packed, x0, st):
+    """Errors of a pairlist and a steady evaluation of frame 0 (the benchmark's
+    flags, no exclusion corrections) against the FP64 oracle (the checker; its
+    evaluation is outside every timed region)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import torch
+    import nbk
+    import oracle
+    o = oracle.Oracle(packed, nbk.NonbondedParams())
+    o.xyzq[:] = x0.cpu().numpy()      # packed holds the trajectory's last frame
+    Fo, So, ro = o.forces(1)
+    real = np.zeros(packed.atomStorageSize, dtype=bool)
+    real[packed.slotOfAtom] = True
+    n = packed.atomStorageSize
+    fixed = torch.zeros((6, n), dtype=torch.int64, device=x0.device)
+    FL = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
+
+    def rms(a, b):
+        return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+    out = {}
+    nb.build_tile_lists(packed, xyzq=x0, stream=st)
+    for name, fl in (("pairlist", FL | nbk.NBK_PAIRLIST), ("steady", FL)):
+        nb.force(packed, fl, xyzq=x0, d_fixed=fixed, stream=st)
+        ve = nb.virial_energy(FL, stream=st)
+        torch.cuda.synchronize(x0.device)
+        X = fixed.cpu().numpy().astype(np.float64) / nbk.FORCE_FIXED_SCALE
+        F, S = X[:3].T, X[3:].T
+        e = {"force_rms": rms(F[real], Fo[real]), "slow_force_rms": rms(S[real], So[real])}
+        for k in ("energyVdw", "energyElec", "energySlow"):
+            e[k] = abs(getattr(ve, k) - ro[k]) / abs(ro[k])
+        e["virial"] = rms(np.array(ve.virial).reshape(3, 3), ro["virial"])
+        e["virialSlow"] = rms(np.array(ve.virialSlow).reshape(3, 3), ro["virialSlow"])
+        e["pairs_equal"] = bool(nb.pair_count(st) == ro["pairs"])
+        out[name] = {k: (float(f"{v:.3e}") if isinstance(v, float) else v) for k, v in e.items()}
+    out["tolerances"] = {"force_rms": 1e-5, "energies": 1e-6, "virials": 1e-6}
+    return out
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     import nbk
@@ -427,6 +540,7 @@ def run_gpu(args, rank, world, local_rank):
     clocks = sampler.stop()
     launches = nb.launch_count() - launches0
     ktimes = nb.kernel_times()
+    ptimes = nb.precise_times()
     nb.set_kernel_timing(False)
     step_ms = np.array([a.elapsed_time(b) for a, b in ev])
     total_ms = float(step_ms.sum())
@@ -434,12 +548,16 @@ def run_gpu(args, rank, world, local_rank):
     total_ms, pairs = combine_ranks(total_ms, pairs, dist, dev)
     value = pairs / (total_ms * 1e-3)
 
-    # dominant kernel: steady-state force kernel (9 of every 10 launches)
+    # dominant kernel: steady-state force kernel (9 of every 10 launches);
+    # then the precise energy / virial kernel (FP64) of the same evaluations
     steady = np.array([ktimes[k] for k in range(len(ktimes)) if k % REBUILD != 0])
     plist = np.array([ktimes[k] for k in range(len(ktimes)) if k % REBUILD == 0])
+    psteady = np.array([ptimes[k] for k in range(len(ptimes)) if k % REBUILD != 0])
     steady_pairs = np.mean([pairs_of[k % NFRAMES] for k in range(args.steps) if k % REBUILD])
     fp32_peak = nbk.measure_fp32_peak(local_rank)
+    fp64_peak = nbk.measure_fp64_peak(local_rank)
     achieved = FLOPS_PER_PAIR * steady_pairs / (steady.mean() * 1e-3) / 1e12
+    achieved64 = FP64_FLOPS_PER_PAIR * steady_pairs / (psteady.mean() * 1e-3) / 1e12
     traffic = None
     if os.path.exists(PROFILE_TRAFFIC):
         try:
@@ -455,8 +573,19 @@ def run_gpu(args, rank, world, local_rank):
                 "kernel": "forceKernel<energy,virial,slow> (steady state)",
                 "kernel_ms": float(steady.mean()), "pairlist_kernel_ms": float(plist.mean()) if len(plist) else None,
                 "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": float(steady_pairs),
+                "traffic_source": ("dram__bytes_read.sum + dram__bytes_write.sum of one steady "
+                                   "launch, from the committed ncu capture " +
+                                   os.path.relpath(PROFILE_TRAFFIC, ROOT)),
                 "hbm_view": {"alg_bytes": alg_bytes,
-                             "achieved_gbs": alg_bytes / (steady.mean() * 1e-3) / 1e9}}
+                             "achieved_gbs": alg_bytes / (steady.mean() * 1e-3) / 1e9},
+                "precise_kernel": {
+                    "kernel": "preciseKernel<energy,virial,slow>: electrostatic energies and "
+                              "slow virial in FP64 per interacting pair",
+                    "bound": "fp64", "achieved": achieved64, "peak": fp64_peak,
+                    "unit": "TFLOP/s", "frac": achieved64 / fp64_peak,
+                    "peak_source": "measured FP64 FMA loop on this GPU (nbk_measure_fp64_peak)",
+                    "kernel_ms": float(psteady.mean()),
+                    "fp64_flops_per_pair": FP64_FLOPS_PER_PAIR}}
 
     # e2e through the C-ABI with host buffers: H2D positions, D2H forces + energies
     pin = torch.from_numpy(frames_h).pin_memory()
@@ -494,6 +623,10 @@ def run_gpu(args, rank, world, local_rank):
     e2e = {"value": e2e_pairs / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 16 * n,
            "d2h_bytes_per_step": 2 * 16 * n + 8 * 31, "steps": ke}
 
+    plain_gpu = None
+    if rank == 0 and world == 1:
+        plain_gpu = reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank,
+                                       value, flush)
     build_t = tile_build_timing(nb, packed, frames[0], stream)
     nb.force(packed, FL | nbk.NBK_PAIRLIST, xyzq=frames[0], d_forces=dF, d_forcesSlow=dS,
              stream=st)
@@ -501,16 +634,22 @@ def run_gpu(args, rank, world, local_rank):
     pme_t = pme_timing(sys_, local_rank, stream)
 
     cpu = None
+    frame0 = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, sample = cpu_eval_sample(packed, args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
                "host": host_cpu()}
+        frame0 = frame0_errors(nb, packed, frames[0], st)
+    legs = {}
+    if rank == 0 and world == 1 and not args.no_legs:
+        legs["batch64"] = batch_leg(50, 3, local_rank)
+        legs["adjoint24k"] = adjoint_leg(20, 3, local_rank)
 
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "atoms": NATOMS, "atom_slots": n,
                        "pairs_per_eval": float(pairs_of.mean()), "rebuild_every": REBUILD,
                        "launch_shape": shape,
@@ -519,6 +658,17 @@ def run_gpu(args, rank, world, local_rank):
             "evals_per_s": args.steps / (total_ms * 1e-3) * world,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(launches), "clocks": clocks,
+            "step_breakdown_ms": {
+                "steady_force_kernel": float(steady.mean()),
+                "steady_precise_kernel": float(psteady.mean()),
+                "pairlist_force_and_refinement": float(plist.mean()) if len(plist) else None,
+                "pairlist_precise_kernel": float(np.mean([ptimes[k] for k in range(len(ptimes))
+                                                          if k % REBUILD == 0]))
+                if len(plist) else None},
+            "frame0_errors_vs_fp64_oracle": frame0,
+            "plain_gpu_path": plain_gpu,
+            "batch64": legs.get("batch64"),
+            "adjoint_ratio": legs.get("adjoint24k"),
             "tile_build": build_t,
             "resident_marshaling": resident,
             "pme_reciprocal": pme_t,
@@ -532,10 +682,12 @@ BATCH_METRIC = ("replica-evals/s, 64 replicas of 2,000-40,000 atoms in one launc
                 "vs one launch per replica")
 
 
-def run_batch(args, rank, world, local_rank):
+def batch_leg(steps, warmup, local_rank, rank=0):
     """64 independent replicas (log-uniform 2k-40k atoms, 0.1 atoms/A^3, own
     seeds): the batched handle's steady-state evaluation captured in a CUDA
-    graph, against the same replicas evaluated one handle and one launch each."""
+    graph, against the same replicas evaluated one handle and one launch
+    sequence each, and against the reference's own kernels, one instance per
+    replica (its plain GPU path), when the reference harness is built."""
     import torch
     import nbk
     dev = torch.device("cuda", local_rank)
@@ -564,7 +716,7 @@ def run_batch(args, rank, world, local_rank):
         nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
         pairs = int(nb.pair_counts(st).sum())
         shape = nb.autotune(FL, iterations=3, stream=st)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             nb.force(many, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
             nb.virial_energy_batch_to(dVE.data_ptr(), True, stream=st)
         stream.synchronize()
@@ -577,16 +729,17 @@ def run_batch(args, rank, world, local_rank):
             g.replay()
         stream.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-              for _ in range(args.steps)]
-        for k in range(args.steps):
+              for _ in range(steps)]
+        for k in range(steps):
             flush.zero_()
             ev[k][0].record(stream)
             g.replay()
             ev[k][1].record(stream)
         stream.synchronize()
         batched_ms = sum(a.elapsed_time(b) for a, b in ev)
+        del g
 
-        # plain path: one handle per replica, one launch sequence per replica
+        # the product's own plain path: one handle per replica
         plain = []
         for r, sy in enumerate(systems):
             pk = nbk.Packed(sy)
@@ -600,40 +753,94 @@ def run_batch(args, rank, world, local_rank):
             h.force(pk, FL | nbk.NBK_PAIRLIST, xyzq=xr, d_forces=fr, d_forcesSlow=sr, stream=st)
             h.autotune(FL, iterations=3, stream=st)
             plain.append((h, pk, xr, fr, sr, ver))
-        ksteps = max(3, min(args.steps, 200))
+        ksteps = max(3, min(steps, 50))
         pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                for _ in range(ksteps)]
-        for k in range(args.warmup + ksteps):
-            if k >= args.warmup:
+        for k in range(warmup + ksteps):
+            if k >= warmup:
                 flush.zero_()
-                pev[k - args.warmup][0].record(stream)
+                pev[k - warmup][0].record(stream)
             for h, pk, xr, fr, sr, ver in plain:
                 h.force(pk, FL, xyzq=xr, d_forces=fr, d_forcesSlow=sr, stream=st)
                 h.virial_energy_to(ver.data_ptr(), True, stream=st)
-            if k >= args.warmup:
-                pev[k - args.warmup][1].record(stream)
+            if k >= warmup:
+                pev[k - warmup][1].record(stream)
         stream.synchronize()
         plain_ms = sum(a.elapsed_time(b) for a, b in pev)
-    batched = 64 * args.steps / (batched_ms * 1e-3)
+        for h, *_ in plain:
+            h.close()
+        nb.close()
+    batched = 64 * steps / (batched_ms * 1e-3)
     plainv = 64 * ksteps / (plain_ms * 1e-3)
+    out = {"value": batched, "unit": "replica-evals/s", "ms_per_step": batched_ms / steps,
+           "steps": steps, "atoms": int(sizes.sum()), "pairs_per_batch_eval": pairs,
+           "launch_shape": shape, "pairs_per_s": pairs * steps / (batched_ms * 1e-3),
+           "product_one_handle_per_replica": {"value": plainv, "unit": "replica-evals/s",
+                                              "ms_per_step": plain_ms / ksteps, "steps": ksteps},
+           "speedup_vs_product_per_replica": batched / plainv}
+    ref = reference_batch(systems, params, warmup, ksteps, local_rank)
+    if ref is not None:
+        out["reference_one_instance_per_replica"] = ref
+        out["speedup_vs_reference_plain_path"] = batched / ref["value"]
+    return out
+
+
+def reference_batch(systems, params, warmup, ksteps, local_rank):
+    """The reference's plain GPU path on the batch: one CudaTileListKernel +
+    CudaComputeNonbondedKernel instance per replica (its texture-table mode,
+    force + energy + virial + slow), steady steps back to back on one stream.
+    None when the reference harness is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refgpu
+    if not refgpu.available():
+        return None
+    import torch
+    import nbk
+    refs = []
+    for sy in systems:
+        pk = nbk.Packed(sy)
+        r = refgpu.RefGpu(params, sy.lj_table(), do_table=1, device=local_rank)
+        r.setup(pk)
+        refs.append((r, np.ascontiguousarray(pk.xyzq)))
+    # one caller stream for all instances (an instance given another stream
+    # gives up its own, so the shared stream must belong to none of them)
+    rs = torch.cuda.Stream(torch.device("cuda", local_rank))
+    for r, x in refs:
+        r.set_stream(rs.cuda_stream)
+        r.eval(1, 1, 1, 1, x)
+    for _ in range(warmup):
+        for r, _x in refs:
+            r.eval(0, 1, 1, 1, None)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(rs)
+    for _ in range(ksteps):
+        for r, _x in refs:
+            r.eval(0, 1, 1, 1, None)
+    e1.record(rs)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / ksteps
+    for r, _x in refs:
+        r.set_stream(0)
+    del refs
+    return {"value": 64 / (ms * 1e-3), "unit": "replica-evals/s", "ms_per_step": ms,
+            "steps": ksteps, "mode": "texture tables (the reference's mode with slow forces)"}
+
+
+def run_batch(args, rank, world, local_rank):
+    out = batch_leg(args.steps, args.warmup, local_rank, rank)
     print(json.dumps({
-        "metric": BATCH_METRIC, "value": batched, "unit": "replica-evals/s", "n_gpus": 1,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batched_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "metric": BATCH_METRIC, "value": out["value"], "unit": "replica-evals/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic",
         "config": {"workload": "batch64: 64 mixed replicas, log-uniform 2,000-40,000 atoms, "
                                "0.1 atoms/A^3, own seeds; steady-state force+energy+virial+slow",
-                   "atoms": int(sizes.sum()), "pairs_per_batch_eval": pairs,
-                   "launch_shape": shape,
-                   "l2": "flushed between timed steps"},
-        "pairs_per_s": pairs * args.steps / (batched_ms * 1e-3),
-        "plain_one_launch_per_replica": {"value": plainv, "unit": "replica-evals/s",
-                                         "ms_per_step": plain_ms / ksteps, "steps": ksteps},
-        "speedup_vs_plain": batched / plainv,
-    }))
+                   "atoms": out["atoms"], "pairs_per_batch_eval": out["pairs_per_batch_eval"],
+                   "launch_shape": out["launch_shape"], "l2": "flushed between timed steps"},
+        "batch": out}))
 
 
-def run_adjoint(args, rank, world, local_rank):
+def adjoint_leg(steps, warmup, local_rank, rank=0):
     """24,000-atom mixed system: the adjoint (gradient of sum w.F + 0.1 E for
     positions, charges and LJ parameters, recomputed from the tile lists)
     against one forward force+energy+virial evaluation of the same lists."""
@@ -662,15 +869,15 @@ def run_adjoint(args, rank, world, local_rank):
     dS = torch.zeros((n, 4), device=dev)
     nb.build_tile_lists(p, xyzq=x, stream=st)
     nb.force(p, FL | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         nb.force(p, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
         nb.adjoint(w, w, 0.1, 0.1, 0.1, g, gab, type_mask=mask, stream=st)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     ev_f = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            for _ in range(args.steps)]
+            for _ in range(steps)]
     ev_a = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-            for _ in range(args.steps)]
-    for k in range(args.steps):
+            for _ in range(steps)]
+    for k in range(steps):
         flush.zero_()
         ev_f[k][0].record(stream)
         nb.force(p, FL, xyzq=x, d_forces=dF, d_forcesSlow=dS, stream=st)
@@ -680,16 +887,23 @@ def run_adjoint(args, rank, world, local_rank):
         nb.adjoint(w, w, 0.1, 0.1, 0.1, g, gab, type_mask=mask, stream=st)
         ev_a[k][1].record(stream)
     torch.cuda.synchronize(dev)
-    fwd = sum(a.elapsed_time(b) for a, b in ev_f) / args.steps
-    adj = sum(a.elapsed_time(b) for a, b in ev_a) / args.steps
+    fwd = sum(a.elapsed_time(b) for a, b in ev_f) / steps
+    adj = sum(a.elapsed_time(b) for a, b in ev_a) / steps
+    nb.close()
+    return {"value": adj / fwd, "unit": "adjoint time / forward time", "steps": steps,
+            "forward_ms": fwd, "adjoint_ms": adj,
+            "workload": "adjoint24k: 24,000-atom mixed system, L = sum w.(F+Fslow) + "
+                        "0.1 (E_vdw+E_elec+E_slow), gradients for positions, charges and the "
+                        "32 solute types' LJ parameters; forward = force+energy+virial+slow"}
+
+
+def run_adjoint(args, rank, world, local_rank):
+    out = adjoint_leg(args.steps, args.warmup, local_rank, rank)
     print(json.dumps({
-        "metric": "adjoint cost / forward cost, 24,000 atoms", "value": adj / fwd, "unit": "ratio",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
-        "data": "synthetic", "dtype": "f32",
-        "config": {"workload": "adjoint24k: 24,000-atom mixed system, L = sum w.(F+Fslow) + "
-                               "0.1 (E_vdw+E_elec+E_slow), gradients for positions, charges and "
-                               "the 32 solute types' LJ parameters"},
-        "forward_ms": fwd, "adjoint_ms": adj}))
+        "metric": "adjoint cost / forward cost, 24,000 atoms", "value": out["value"],
+        "unit": "ratio", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": False, "data": "synthetic", "dtype": "f32+f64",
+        "config": {"workload": out["workload"]}, "adjoint": out}))
 
 
 def main():
@@ -700,6 +914,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-legs", action="store_true",
+                    help="skip the batch64 and adjoint24k legs of the default run")
     ap.add_argument("--workload", choices=["mixed92k", "batch64", "adjoint24k", "large1m"],
                     default="mixed92k",
                     help="batch64: 64-replica batched launch vs one launch per replica; "

@@ -337,10 +337,15 @@ NBK_API int nbk_slow_table(double ewaldcof, double cutoff, double pairlistdist, 
 /* Enables (1) or disables (0) CUDA-event timing of every force-kernel launch
  * of this handle; enabling clears the recorded launches. */
 NBK_API int nbk_set_kernel_timing(nbk_handle h, int enable);
-/* Durations (ms) of the force-kernel launches recorded since timing was
- * enabled, oldest first (synchronises). *count receives the number recorded
- * (at most 4096 are kept); at most maxCount are written. */
+/* Durations (ms) of the evaluations recorded since timing was enabled,
+ * oldest first (synchronises): the force kernel, with the refinement,
+ * compaction and sort before it on pairlist evaluations. *count receives the
+ * number recorded (at most 4096 are kept); at most maxCount are written. */
 NBK_API int nbk_get_kernel_times(nbk_handle h, float* ms, int maxCount, int* count);
+/* The same evaluations' precise energy / virial kernel (the FP64 pass after
+ * the force kernel on evaluations with NBK_ENERGY, or NBK_VIRIAL | NBK_SLOW;
+ * about 0 otherwise). */
+NBK_API int nbk_get_precise_times(nbk_handle h, float* ms, int maxCount, int* count);
 /* Pairs evaluated within the cutoff by the last nbk_nonbonded_force, which
  * must have had NBK_ENERGY (the work unit of the pairs/s metric; synchronises). */
 NBK_API int nbk_get_pair_count(nbk_handle h, long long* pairs, void* stream);
@@ -349,6 +354,8 @@ NBK_API long long nbk_launch_count(nbk_handle h);
 /* FP32 FMA throughput of the device (TFLOP/s, FMA = 2 flops), measured with a
  * register-resident FMA loop over all SMs (synchronises; ~50 ms). */
 NBK_API int nbk_measure_fp32_peak(int deviceID, double* tflops);
+/* FP64 FMA throughput of the device, measured the same way. */
+NBK_API int nbk_measure_fp64_peak(int deviceID, double* tflops);
 
 /* Autotuner of the force kernel's launch shape (no counterpart in the
  * reference, whose launch shape is fixed: NONBONDKERNEL_NUM_WARP warps per

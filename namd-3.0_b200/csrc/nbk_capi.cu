@@ -158,18 +158,22 @@ struct nbk_context {
   // measurement
   long long launches = 0;
   bool timing = false;
-  std::vector<cudaEvent_t> evStart, evStop;
+  std::vector<cudaEvent_t> evStart, evMid, evStop;
   int numTimed = 0;
 };
 
 namespace {
 constexpr int kMaxTimed = 4096;
 
-// Records an event pair around the force-kernel launch when timing is on.
-cudaError_t timedEvent(nbk_context* h, bool start, cudaStream_t st) {
+// Records the events of one evaluation when timing is on: before the force
+// kernel (and the pairlist work before it), between the force kernel and the
+// precise energy / virial kernel, and after that.
+enum TimedPoint { kTimedStart = 0, kTimedMid = 1, kTimedStop = 2 };
+cudaError_t timedEvent(nbk_context* h, TimedPoint which, cudaStream_t st) {
   if (!h->timing) return cudaSuccess;
   const int k = h->numTimed % kMaxTimed;
-  std::vector<cudaEvent_t>& v = start ? h->evStart : h->evStop;
+  std::vector<cudaEvent_t>& v =
+      which == kTimedStart ? h->evStart : (which == kTimedMid ? h->evMid : h->evStop);
   if ((int)v.size() <= k) {
     cudaEvent_t e;
     cudaError_t r = cudaEventCreate(&e);
@@ -177,7 +181,7 @@ cudaError_t timedEvent(nbk_context* h, bool start, cudaStream_t st) {
     v.push_back(e);
   }
   cudaError_t r = cudaEventRecord(v[k], st);
-  if (!start) ++h->numTimed;
+  if (which == kTimedStop) ++h->numTimed;
   return r;
 }
 }  // namespace
@@ -611,7 +615,7 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   ForceArgs a = refinedForceArgs(h, cutoff2);
   const int key = tuneKey(h, flags);
   a.splitLog2 = h->tuneSplitLog2[key];
-  NBK_CUDA(timedEvent(h, true, st), "timing event");
+  NBK_CUDA(timedEvent(h, kTimedStart, st), "timing event");
   if (pairlist) {
     // refinement of the culled lists (the pairlist pass), then their
     // compaction (reSortTileLists), both on the device
@@ -657,13 +661,14 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   }
   NBK_CUDA(launchForce(a, flags, h->tuneMinBlocks[key], h->numSM, st), "force kernel");
   h->launches += 1;
+  NBK_CUDA(timedEvent(h, kTimedMid, st), "timing event");
   if (needsPrecise(flags)) {
     ForceArgs pa = a;
     pa.workCounter = h->counters.p + 4;
     NBK_CUDA(launchPrecise(pa, flags, h->numSM, st), "precise energy / virial kernel");
     h->launches += 1;
   }
-  NBK_CUDA(timedEvent(h, false, st), "timing event");
+  NBK_CUDA(timedEvent(h, kTimedStop, st), "timing event");
   if ((flags & NBK_CORRECTIONS) && (h->numMod || h->numExc)) {
     if (h->maxTupleSlot >= n)
       return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: a correction tuple names a slot beyond atomStorageSize");
@@ -840,9 +845,10 @@ NBK_API int nbk_adjoint(nbk_handle h, unsigned flags, const nbk_float4* d_wF, co
   a.stride = n;
   a.gradAB = d_gradAB;
   a.workCounter = h->counters.p + 2;
-  NBK_CUDA(timedEvent(h, true, st), "timing event");
+  NBK_CUDA(timedEvent(h, kTimedStart, st), "timing event");
   NBK_CUDA(launchAdjoint(a, slow, h->numSM, n, reinterpret_cast<float4*>(d_gradXQ), st), "adjoint kernel");
-  NBK_CUDA(timedEvent(h, false, st), "timing event");
+  NBK_CUDA(timedEvent(h, kTimedMid, st), "timing event");
+  NBK_CUDA(timedEvent(h, kTimedStop, st), "timing event");
   h->launches += d_gradXQ ? 2 : 1;
   if (d_gradFixed)
     NBK_CUDA(cudaMemcpyAsync(d_gradFixed, h->adjGrad.p, sizeof(long long) * 4 * (size_t)n,
@@ -945,19 +951,33 @@ NBK_API int nbk_set_kernel_timing(nbk_handle h, int enable) {
   return NBK_OK;
 }
 
-NBK_API int nbk_get_kernel_times(nbk_handle h, float* ms, int maxCount, int* count) {
-  int rc = checkHandle(h, "nbk_get_kernel_times");
+namespace {
+int timesBetween(nbk_handle h, const std::vector<cudaEvent_t>& from,
+                 const std::vector<cudaEvent_t>& to, float* ms, int maxCount, int* count,
+                 const char* fn) {
+  int rc = checkHandle(h, fn);
   if (rc) return rc;
-  if (!count || (maxCount > 0 && !ms)) return setErr(NBK_ERR_ARG, "nbk_get_kernel_times: NULL output");
+  if (!count || (maxCount > 0 && !ms)) return setErr(NBK_ERR_ARG, std::string(fn) + ": NULL output");
   const int n = std::min(h->numTimed, kMaxTimed);
   *count = n;
   const int first = h->numTimed - n;
   for (int k = 0; k < n && k < maxCount; ++k) {
     const int slot = (first + k) % kMaxTimed;
-    NBK_CUDA(cudaEventSynchronize(h->evStop[slot]), "nbk_get_kernel_times");
-    NBK_CUDA(cudaEventElapsedTime(&ms[k], h->evStart[slot], h->evStop[slot]), "nbk_get_kernel_times");
+    NBK_CUDA(cudaEventSynchronize(to[slot]), fn);
+    NBK_CUDA(cudaEventElapsedTime(&ms[k], from[slot], to[slot]), fn);
   }
   return NBK_OK;
+}
+}  // namespace
+
+NBK_API int nbk_get_kernel_times(nbk_handle h, float* ms, int maxCount, int* count) {
+  if (!h) return setErr(NBK_ERR_ARG, "nbk_get_kernel_times: NULL handle");
+  return timesBetween(h, h->evStart, h->evMid, ms, maxCount, count, "nbk_get_kernel_times");
+}
+
+NBK_API int nbk_get_precise_times(nbk_handle h, float* ms, int maxCount, int* count) {
+  if (!h) return setErr(NBK_ERR_ARG, "nbk_get_precise_times: NULL handle");
+  return timesBetween(h, h->evMid, h->evStop, ms, maxCount, count, "nbk_get_precise_times");
 }
 
 NBK_API long long nbk_launch_count(nbk_handle h) { return h ? h->launches : -1; }
@@ -1000,6 +1020,57 @@ __global__ void fmaPeakKernel(int iters, float seed, float* out) {
   if (s == 12345.678f) out[0] = s;  // never true; keeps the chains alive
 }
 }  // namespace
+
+namespace {
+// The same with FP64 FMAs.
+__global__ void dfmaPeakKernel(int iters, double seed, double* out) {
+  double a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4,
+         a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+  const double m = 0.999999, c = 1e-7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+    }
+  }
+  if (a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7 == -1.0) *out = a0;  // keeps the chains live
+}
+}  // namespace
+
+extern "C" NBK_API int nbk_measure_fp64_peak(int deviceID, double* tflops) {
+  if (!tflops) return setErr(NBK_ERR_ARG, "nbk_measure_fp64_peak: NULL output");
+  NBK_CUDA(cudaSetDevice(deviceID), "nbk_measure_fp64_peak");
+  cudaDeviceProp prop;
+  NBK_CUDA(cudaGetDeviceProperties(&prop, deviceID), "nbk_measure_fp64_peak");
+  double* out = nullptr;
+  NBK_CUDA(cudaMalloc(&out, sizeof(double)), "nbk_measure_fp64_peak");
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int threads = 256, blocks = prop.multiProcessorCount * 8, iters = 1024;
+  dfmaPeakKernel<<<blocks, threads>>>(16, 1.0, out);  // warm-up
+  double best = 0;
+  for (int rep = 0; rep < 3; ++rep) {
+    cudaEventRecord(e0);
+    dfmaPeakKernel<<<blocks, threads>>>(iters, 1.0, out);
+    cudaEventRecord(e1);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e != cudaSuccess) {
+      cudaFree(out);
+      return setErr(NBK_ERR_CUDA, std::string("nbk_measure_fp64_peak: ") + cudaGetErrorString(e));
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+    best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  *tflops = best;
+  return NBK_OK;
+}
 
 extern "C" NBK_API int nbk_measure_fp32_peak(int deviceID, double* tflops) {
   if (!tflops) return setErr(NBK_ERR_ARG, "nbk_measure_fp32_peak: NULL output");

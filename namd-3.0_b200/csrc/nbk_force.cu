@@ -130,12 +130,12 @@ __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable&
   double p = 0.0, dp = 0.0;
   if (doSlow) {
     // row k = nearest integer to s/D: adding 1.5 * 2^52 rounds s/D (exact, D
-    // a power of two) into the low word; the sum is clamped to the last row
-    // in FP64, so k and w = s - k D come without an integer conversion
+    // a power of two) into the low word; k is clamped to the last row (any
+    // bit pattern stays in the table) and w = s - k D
     const double magic = 6755399441055744.0;
-    const double t = fmin(fma(s, T.invStep, magic), magic + (double)T.last);
-    const unsigned k = (unsigned)__double2loint(t);
-    const double wq = fma(-T.step, t - magic, s);
+    const double t = fma(s, T.invStep, magic);
+    const unsigned k = min((unsigned)__double2loint(t), T.last);
+    const double wq = fma(-T.step, (double)k, s);
     double cf[kSlowTableDeg1];
 #pragma unroll
     for (int n = 0; n < kSlowTableDeg1; n += 2) {
@@ -173,19 +173,36 @@ __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable&
   }
 }
 
+// Queue entry e of the precise pass as FP64 pair terms; every lane takes
+// part in the shuffles. An entry past the end (e >= total) repeats entry 0, a
+// real pair (its atoms are distinct, so its distance is not 0), with qq = 0,
+// which contributes exact zeros.
+__device__ __forceinline__ void loadPair(const unsigned short* q, const int e, const int total,
+                                         const double4 ai, const double4 aj, PairTerms& u) {
+  const bool valid = e < total;
+  const unsigned ent = q[valid ? e : 0];
+  const int i = ent & 31, j = (i + (ent >> 5)) & 31;
+  const double ax = __shfl_sync(0xffffffffu, ai.x, i), ay = __shfl_sync(0xffffffffu, ai.y, i),
+               az = __shfl_sync(0xffffffffu, ai.z, i), aq = __shfl_sync(0xffffffffu, ai.w, i);
+  const double bx = __shfl_sync(0xffffffffu, aj.x, j), by = __shfl_sync(0xffffffffu, aj.y, j),
+               bz = __shfl_sync(0xffffffffu, aj.z, j), bq = __shfl_sync(0xffffffffu, aj.w, j);
+  u.dx = bx - ax;
+  u.dy = by - ay;
+  u.dz = bz - az;
+  u.qq = valid ? aq * bq : 0.0;
+}
+
 // The precise pass of one tile. live (per lane): bit t set when the pair
 // (i = lane, j = (lane + t) & 31) is an interacting pair (mask bit set and
 // FP32 r^2 below the cutoff, the classification the FP32 math used). The
 // warp compacts the tile's interacting pairs into a queue in shared memory
 // (entry = i | t << 5, lane-major order; at most 32 * 32 two-byte entries,
 // the 2 KB of pq) and processes them in FP64, two per lane per iteration
-// (entries e and e + 32: independent dependency chains). Lane l holds atom l
-// of the list's i tile (ai: the FP64 shifted position and charge) and of the
-// current j tile (aj, FP64), and a pair's atoms come by shuffles. An entry
-// past the end gets d = (1, 0, 0) and qq = 0, which contributes exact zeros
-// (its atoms may be one and the same atom, so their own distance, 0, would
-// turn the zero into a NaN). Every step is warp-synchronous and the sums
-// depend only on the tile group.
+// (entries e and e + 32: independent dependency chains) while more than 32
+// remain, then one. Lane l holds atom l of the list's i tile (ai: the FP64
+// shifted position and charge) and of the current j tile (aj, FP64), and a
+// pair's atoms come by shuffles (loadPair). Every step is warp-synchronous
+// and the sums depend only on the tile group.
 template <bool doEnergy, bool doVirial, bool doSlow, int kCopies>
 __device__ __forceinline__ void precisePass(const unsigned live, const int lane, const double4 ai,
                                             const double4 aj, double* pq, const SlowTable& T,
@@ -215,26 +232,19 @@ __device__ __forceinline__ void precisePass(const unsigned live, const int lane,
     pos += 2;
   }
   __syncwarp();
-  for (int base = 0; base < total; base += 2 * kWarp) {  // warp-uniform
+  // two entries per lane per iteration while more than 32 remain, then one
+  int base = 0;
+  for (; total - base > kWarp; base += 2 * kWarp) {  // warp-uniform
     PairTerms u[2];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int e = base + h * kWarp + lane;
-      const bool valid = e < total;
-      const unsigned ent = valid ? q[e] : 0u;
-      const int i = ent & 31, j = (i + (ent >> 5)) & 31;
-      // every lane takes part in the shuffles
-      const double ax = __shfl_sync(0xffffffffu, ai.x, i), ay = __shfl_sync(0xffffffffu, ai.y, i),
-                   az = __shfl_sync(0xffffffffu, ai.z, i), aq = __shfl_sync(0xffffffffu, ai.w, i);
-      const double bx = __shfl_sync(0xffffffffu, aj.x, j), by = __shfl_sync(0xffffffffu, aj.y, j),
-                   bz = __shfl_sync(0xffffffffu, aj.z, j), bq = __shfl_sync(0xffffffffu, aj.w, j);
-      u[h].dx = valid ? bx - ax : 1.0;
-      u[h].dy = valid ? by - ay : 0.0;
-      u[h].dz = valid ? bz - az : 0.0;
-      u[h].qq = valid ? aq * bq : 0.0;
-    }
+    for (int h = 0; h < 2; ++h) loadPair(q, base + h * kWarp + lane, total, ai, aj, u[h]);
 #pragma unroll
     for (int h = 0; h < 2; ++h) precisePair<doEnergy, doVirial, doSlow, kCopies>(u[h], T, c, lane, L);
+  }
+  if (base < total) {  // warp-uniform
+    PairTerms u;
+    loadPair(q, base + lane, total, ai, aj, u);
+    precisePair<doEnergy, doVirial, doSlow, kCopies>(u, T, c, lane, L);
   }
   __syncwarp();  // the queue is consumed before pq is written again
 }

@@ -96,7 +96,7 @@ __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
 
 // erfc(x) = t P(t) exp(-x^2), t = 1/(1 + p x): Hastings' rational form (the
 // form of Abramowitz & Stegun 7.1.26) with a degree-7 P whose coefficients
-// were fitted by least squares on [0, 4] (fit_erfc.py; max relative error
+// were fitted by least squares on [0, 4] (oracle/fit_erfc.py; max relative error
 // 1.6e-8). `ex` is exp(-x^2), shared with the force's Gaussian term.
 constexpr float kErfcP = 4.067848869e-01f;
 constexpr float kErfcC0 = 8.043135869e-02f, kErfcC1 = -4.030445941e-01f,

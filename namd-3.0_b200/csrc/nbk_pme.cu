@@ -57,8 +57,10 @@ double reciprocal(const double* L, Recip& R) {
   return vol;
 }
 
-// B-spline weights theta_k(w), k = 0..order-1, by the recursion of the
-// reference (order 2 from w, raised one order at a time).
+// B-spline weights theta_k(w), k = 0..order-1, by the cardinal B-spline
+// recursion of smooth PME (Essmann et al., J. Chem. Phys. 103, 8577 (1995),
+// eq. 4.1; the reference's calc_one_theta, src/CudaPmeSolverUtilKernel.cu:
+// 331-359, uses the same): order 2 from w, raised one order at a time.
 template <typename T, int order>
 __host__ __device__ __forceinline__ void bsplineTheta(const T w, T* theta) {
   theta[order - 1] = T(0);

@@ -359,6 +359,8 @@ def dev_lib() -> C.CDLL:
         lib.nbk_launch_count.argtypes = [vp]
         lib.nbk_get_pair_count.argtypes = [vp, C.POINTER(C.c_longlong), vp]
         lib.nbk_measure_fp32_peak.argtypes = [i, C.POINTER(C.c_double)]
+        lib.nbk_measure_fp64_peak.argtypes = [i, C.POINTER(C.c_double)]
+        lib.nbk_get_precise_times.argtypes = [vp, C.POINTER(C.c_float), i, C.POINTER(i)]
         lib.nbk_slow_table.argtypes = [C.c_double, C.c_double, C.c_double, vp, i,
                                        C.POINTER(C.c_double)]
         lib.nbk_set_replicas.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, vp, vp]
@@ -553,14 +555,22 @@ class Nonbonded:
     def set_kernel_timing(self, enable: bool):
         _dcheck(dev_lib().nbk_set_kernel_timing(self._h, int(enable)), "nbk_set_kernel_timing")
 
-    def kernel_times(self):
+    def _times(self, fn):
         n = C.c_int(0)
-        _dcheck(dev_lib().nbk_get_kernel_times(self._h, None, 0, C.byref(n)),
-                "nbk_get_kernel_times")
+        f = getattr(dev_lib(), fn)
+        _dcheck(f(self._h, None, 0, C.byref(n)), fn)
         ms = (C.c_float * max(n.value, 1))()
-        _dcheck(dev_lib().nbk_get_kernel_times(self._h, ms, n.value, C.byref(n)),
-                "nbk_get_kernel_times")
+        _dcheck(f(self._h, ms, n.value, C.byref(n)), fn)
         return np.array(ms[:n.value], dtype=np.float64)
+
+    def kernel_times(self):
+        """Per recorded evaluation: the force kernel (with the pairlist work
+        before it on pairlist evaluations), ms."""
+        return self._times("nbk_get_kernel_times")
+
+    def precise_times(self):
+        """Per recorded evaluation: the precise energy / virial kernel, ms."""
+        return self._times("nbk_get_precise_times")
 
     def launch_count(self) -> int:
         return int(dev_lib().nbk_launch_count(self._h))
@@ -655,6 +665,12 @@ def slow_table(ewaldcof: float, cutoff: float, pairlistdist: float):
 def measure_fp32_peak(device: int = 0) -> float:
     t = C.c_double(0)
     _dcheck(dev_lib().nbk_measure_fp32_peak(device, C.byref(t)), "nbk_measure_fp32_peak")
+    return float(t.value)
+
+
+def measure_fp64_peak(device: int = 0) -> float:
+    t = C.c_double(0)
+    _dcheck(dev_lib().nbk_measure_fp64_peak(device, C.byref(t)), "nbk_measure_fp64_peak")
     return float(t.value)
 
 

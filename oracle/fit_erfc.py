@@ -4,7 +4,8 @@ Form (Hastings' rational approximation, the form of Abramowitz & Stegun
 7.1.26):   erfc(x) = t * P(t) * exp(-x^2),  t = 1 / (1 + p x),  x in [0, 4]
 with P a polynomial of degree 7. p and the coefficients are fitted here by
 weighted least squares on the relative error (exact erfc from scipy); the
-printed constants are the ones in csrc/nbk_internal.cuh. Max relative error of
+printed constants are the ones in namd-3.0_b200/csrc/nbk_internal.cuh (kept
+here beside the oracle as their provenance). Max relative error of
 the fit: 1.6e-8, below FP32 resolution. The kernels share exp(-x^2) between
 erfc and the force's Gaussian term, so erfc costs one reciprocal and 8 FMAs.
 
