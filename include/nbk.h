@@ -39,7 +39,6 @@ extern "C" {
 #define NBK_ERR_NOMEM (-4)     /* device or host allocation failed          */
 #define NBK_ERR_OVERFLOW (-5)  /* a size limit of the tile lists was exceeded */
 #define NBK_ERR_DEVICE (-6)    /* no usable sm_100 device                     */
-#define NBK_ERR_TIMEOUT (-7)   /* a bounded device-side wait gave up          */
 
 /* ---- flags for nbk_nonbonded_force / nbk_reduce_virial_energy -------- */
 #define NBK_ENERGY 1u      /* doEnergy   (src/CudaComputeNonbondedKernel.cu:2076) */
@@ -180,7 +179,11 @@ NBK_API int nbk_update_vdw_types_excl(nbk_handle h, int atomStorageSize, const i
  * lists. xyzq is a host pointer (xyzqOnDevice = 0, copied on `stream`) or a
  * device pointer kept by reference (xyzqOnDevice = 1; it must stay valid
  * until the next build). No host synchronisation: capacities are exact upper
- * bounds computed from the patch records. */
+ * bounds computed from the patch records. A patch with more 32-atom tiles than
+ * maxTileListLen, or maxTileListLen >= 65536, returns NBK_ERR_OVERFLOW and sets
+ * tilesSizeExceeded in the TileListStat (the reference's tilesSizeExceeded,
+ * src/CudaTileListKernel.cu:505-509; it reallocates and rebuilds, the caller
+ * here rebuilds with a larger maxTileListLen). */
 NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSize,
                                  int maxTileListLen, nbk_float3 lata, nbk_float3 latb,
                                  nbk_float3 latc, const nbk_patch_record* h_patches,
@@ -331,6 +334,16 @@ NBK_API const char* nbk_noalloc_last_error(void);
  * NBK_ERR_ARG for bad parameters. */
 NBK_API int nbk_slow_table(double ewaldcof, double cutoff, double pairlistdist, double* out,
                            int maxRows, double* step);
+
+/* ---- test hooks -------------------------------------------------------------- */
+
+/* Allocation-failure injection for tests of the error paths: the
+ * countdown-th device allocation made for any handle from now on (counting
+ * the buffers that nbk_create, nbk_update_*, nbk_build_tile_lists,
+ * nbk_nonbonded_force ... grow) fails as an out-of-memory cudaMalloc would,
+ * and the call that made it returns NBK_ERR_NOMEM; later calls allocate
+ * normally. 0 disarms. Process-wide. */
+NBK_API int nbk_debug_fail_alloc(int countdown);
 
 /* ---- measurement ----------------------------------------------------------- */
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,12 +36,20 @@ int setErr(int code, const std::string& msg) {
   return code;
 }
 
+// A failed CUDA call becomes NBK_ERR_NOMEM when it was an allocation that
+// ran out of memory, else NBK_ERR_CUDA.
 #define NBK_CUDA(call, what)                                                              \
   do {                                                                                    \
     cudaError_t e_ = (call);                                                              \
     if (e_ != cudaSuccess)                                                                \
-      return setErr(NBK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_));    \
+      return setErr(e_ == cudaErrorMemoryAllocation ? NBK_ERR_NOMEM : NBK_ERR_CUDA,       \
+                    std::string(what) + ": " + cudaGetErrorString(e_));                   \
   } while (0)
+
+// Allocation-failure injection for tests (nbk_debug_fail_alloc): when > 0,
+// counts down on every device allocation of a handle's buffers, and the
+// allocation that takes it to 0 fails as an out-of-memory cudaMalloc would.
+std::atomic<int> g_failAllocCountdown{0};
 
 // Grow-only device buffer (over-allocates by 20% like the reference's
 // reallocate_device with OVERALLOC, src/CudaTileListKernel.cu:30).
@@ -53,6 +62,10 @@ struct DBuf {
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
+    int c = g_failAllocCountdown.load();
+    while (c > 0 && !g_failAllocCountdown.compare_exchange_weak(c, c - 1)) {
+    }
+    if (c == 1) return cudaErrorMemoryAllocation;
     const size_t want = std::max<size_t>(n + n / 5, 32);
     cudaError_t e = cudaMalloc(&p, want * sizeof(T));
     if (e == cudaSuccess) cap = want;
@@ -124,6 +137,7 @@ struct nbk_context {
   DBuf<unsigned> live;  // [j tiles][32] interacting-pair words of the last energy / virial evaluation
   bool built = false;     // tile lists built (sparse)
   bool refined = false;   // compacted lists valid
+  bool tilesSizeExceeded = false;  // the last build was refused for a size limit
   float3 lata{}, latb{}, latc{};
   // accumulators
   DBuf<long long> force;
@@ -273,6 +287,12 @@ int nbk::setLastError(int code, const std::string& msg) { return setErr(code, ms
 extern "C" {
 
 NBK_API const char* nbk_last_error(void) { return g_err.c_str(); }
+
+NBK_API int nbk_debug_fail_alloc(int countdown) {
+  if (countdown < 0) return setErr(NBK_ERR_ARG, "nbk_debug_fail_alloc: countdown must be >= 0");
+  g_failAllocCountdown.store(countdown);
+  return NBK_OK;
+}
 NBK_API int nbk_version(void) { return 1; }
 
 NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
@@ -320,7 +340,9 @@ NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
   }
   int rc = NBK_OK;
   auto fin = [&](cudaError_t e, const char* what) {
-    if (rc == NBK_OK && e != cudaSuccess) rc = setErr(NBK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    if (rc == NBK_OK && e != cudaSuccess)
+      rc = setErr(e == cudaErrorMemoryAllocation ? NBK_ERR_NOMEM : NBK_ERR_CUDA,
+                  std::string(what) + ": " + cudaGetErrorString(e));
   };
   fin(h->ljTable.ensure(dim * dim), "nbk_create: alloc");
   fin(h->ljExclTable.ensure(dim * dim), "nbk_create: alloc");
@@ -490,8 +512,11 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
   cudaStream_t st = (cudaStream_t)stream;
   if (numPatches <= 0 || !hp || atomStorageSize <= 0 || (atomStorageSize & 31))
     return setErr(NBK_ERR_ARG, "nbk_build_tile_lists: bad argument");
-  if (maxTileListLen >= 65536)
+  if (maxTileListLen >= 65536) {
+    h->tilesSizeExceeded = true;
     return setErr(NBK_ERR_OVERFLOW, "nbk_build_tile_lists: maximum number of tiles per tile list (65536) blown");
+  }
+  if (maxTileListLen <= 0) return setErr(NBK_ERR_ARG, "nbk_build_tile_lists: maxTileListLen must be positive");
   if (h->atomDataSize < atomStorageSize)
     return setErr(NBK_ERR_STATE, "nbk_build_tile_lists: nbk_update_vdw_types_excl not called for this atom storage size");
   if (!h->numComputes) return setErr(NBK_ERR_STATE, "nbk_build_tile_lists: no computes");
@@ -502,8 +527,10 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
     if (r.numAtoms < 0 || r.numFreeAtoms < 0 || r.numFreeAtoms > r.numAtoms || (r.atomStart & 31) ||
         r.atomStart < 0 || r.atomStart + ((r.numAtoms + 31) / 32) * 32 > atomStorageSize)
       return setErr(NBK_ERR_ARG, "nbk_build_tile_lists: patch record out of range of the atom storage");
-    if ((r.numAtoms + 31) / 32 > maxTileListLen)
-      return setErr(NBK_ERR_ARG, "nbk_build_tile_lists: a patch has more tiles than maxTileListLen");
+    if ((r.numAtoms + 31) / 32 > maxTileListLen) {
+      h->tilesSizeExceeded = true;
+      return setErr(NBK_ERR_OVERFLOW, "nbk_build_tile_lists: a patch has more tiles than maxTileListLen");
+    }
     if (same && (r.numAtoms != h->hPatches[p].numAtoms || r.atomStart != h->hPatches[p].atomStart ||
                  r.numFreeAtoms != h->hPatches[p].numFreeAtoms))
       same = false;
@@ -570,6 +597,7 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
   h->c.plcutoff2 = plcutoff2;
   h->built = true;
   h->refined = false;
+  h->tilesSizeExceeded = false;
   return NBK_OK;
 }
 
@@ -767,6 +795,7 @@ NBK_API int nbk_get_tile_list_stat(nbk_handle h, nbk_tile_list_stat* out, void* 
   long long nex = 0;
   for (int r = 0; r < accBlocks; ++r) nex += accHost[(size_t)r * kAccCount + kAccNumExcl];
   std::memset(out, 0, sizeof(*out));
+  out->tilesSizeExceeded = h->tilesSizeExceeded ? 1 : 0;
   out->numTileLists = h->refined ? cnt[0] : h->numLists;
   out->numTileListsGBIS = out->numTileLists;
   out->numJtiles = h->refined ? cnt[1] : h->jcap;

@@ -360,6 +360,7 @@ def dev_lib() -> C.CDLL:
         lib.nbk_get_pair_count.argtypes = [vp, C.POINTER(C.c_longlong), vp]
         lib.nbk_measure_fp32_peak.argtypes = [i, C.POINTER(C.c_double)]
         lib.nbk_measure_fp64_peak.argtypes = [i, C.POINTER(C.c_double)]
+        lib.nbk_debug_fail_alloc.argtypes = [i]
         lib.nbk_get_precise_times.argtypes = [vp, C.POINTER(C.c_float), i, C.POINTER(i)]
         lib.nbk_slow_table.argtypes = [C.c_double, C.c_double, C.c_double, vp, i,
                                        C.POINTER(C.c_double)]

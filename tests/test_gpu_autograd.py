@@ -135,7 +135,8 @@ def case():
     L = (wt * F).sum() + (wt * S).sum() + COT * E.sum()
     (g,) = torch.autograd.grad(L, x)
     gab = run.gradAB.cpu().numpy()
-    return dict(system=s, packed=p, w=w, run=run, L=float(L), grad=g.cpu().numpy(), gab=gab)
+    return dict(system=s, packed=p, w=w, run=run, L=float(L.detach()), grad=g.cpu().numpy(),
+                gab=gab)
 
 
 def test_autograd_gradient_matches_the_fp64_oracle(case):
