@@ -323,10 +323,11 @@ NBK_API const char* nbk_noalloc_last_error(void);
 /* No counterpart in the reference (its slow term comes from interpolated
  * texture tables, src/CudaNonbondedTables.C:158-303). The FP64 slow-term table
  * the precise energy / virial kernel evaluates. With step D (*step; a power
- * of two, 32 A^2 or less, chosen so that the fit is within FP64 rounding),
- * row k (8 doubles) holds the degree-7 Chebyshev interpolant of
- * phi_s(s) = (3 - s/rc^2)/(2 rc) - erf(ewaldcof sqrt(s))/sqrt(s), s = r^2, on
- * s in [k D - D/2, k D + D/2], as coefficients c0..c7 of powers of (s - k D).
+ * of two, 32 A^2 or less, chosen so that the fit is within 1e-12 of
+ * max |phi_s| + 1/rc), row k (6 doubles) holds the degree-5 Chebyshev
+ * interpolant of phi_s(s) = (3 - s/rc^2)/(2 rc) - erf(ewaldcof sqrt(s))/sqrt(s),
+ * s = r^2, on s in [k D - D/2, k D + D/2], as coefficients c0..c5 of powers of
+ * (s - k D).
  * The slow pair energy is qq phi_s(s), the slow force factor
  * (dE/dr)/r = 2 qq phi_s'(s). Rows cover s up to pairlistdist^2 + 2.
  * Host-only (no GPU needed): returns the number of rows and, when out is not

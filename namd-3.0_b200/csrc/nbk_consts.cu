@@ -84,8 +84,8 @@ static double slowPhi(double beta, double rc, double s) {
   return (3.0 - s / (rc * rc)) / (2.0 * rc) - erfOverR(beta, s);
 }
 
-// One table of the given power-of-two step: row k the degree-7 Chebyshev
-// interpolant (8 nodes) on s in [k step - step/2, k step + step/2] written in
+// One table of the given power-of-two step: row k the degree-5 Chebyshev
+// interpolant (6 nodes) on s in [k step - step/2, k step + step/2] written in
 // powers of w = s - k step. Returns the largest deviation from phi_s at 32
 // points per row between the nodes.
 static double fitSlowTable(double beta, double rc, double step, int rows, std::vector<double>& out) {
@@ -125,9 +125,9 @@ static double fitSlowTable(double beta, double rc, double step, int rows, std::v
 
 // The slow-term table of the precise pass (layout in nbk_internal.cuh), over
 // s in [0, pairlistdist^2 + 2]. The step starts at 32 A^2 and is halved
-// (down to 1/32 of that) until the fit is within 4e-15 of max |phi_s| (the
-// interpolation error of a row grows as (beta^2 step)^8). Returns the number
-// of rows; *stepOut receives the step.
+// (down to 1/128 of that) until the fit is within kSlowTableTol of
+// max |phi_s| + 1/rc (the interpolation error of a row grows as
+// (beta^2 step)^6). Returns the number of rows; *stepOut receives the step.
 int buildSlowTable(double beta, double cutoff, double pairlistdist, std::vector<double>& out,
                    double* stepOut) {
   const double smax = pairlistdist * pairlistdist + 2.0;
@@ -137,7 +137,7 @@ int buildSlowTable(double beta, double cutoff, double pairlistdist, std::vector<
   for (;;) {
     rows = (int)std::ceil(smax / step + 0.5) + 1;
     const double err = fitSlowTable(beta, cutoff, step, rows, out);
-    if (err <= 4e-15 * scale || step <= kSlowTableStepMax / 32) break;
+    if (err <= kSlowTableTol * scale || step <= kSlowTableStepMax / 128) break;
     step *= 0.5;
   }
   if (stepOut) *stepOut = step;

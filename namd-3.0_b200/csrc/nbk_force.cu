@@ -40,11 +40,6 @@ constexpr int kForceThreads = kForceWarps * kWarp;
 // independent components of the slow virial (xx, xy, xz, yy, yz, zz).
 constexpr int kQElec = 0, kQSlow = 1, kQVir = 2, kNumQ = 8;
 
-// An atom in FP64 (position, scaled charge); 32 bytes, two 16-byte loads.
-struct alignas(16) Atom64 {
-  double x, y, z, q;
-};
-
 // virialSlow[3a+b] slots of symmetric component m (xx, xy, xz, yy, yz, zz);
 // s1 < 0 for the diagonal.
 __device__ __forceinline__ void symSlots(int m, int& s0, int& s1) {
@@ -90,6 +85,16 @@ struct PairTerms {
   double dx, dy, dz, qq;
 };
 
+// The warp's atoms in FP64 as the precise pass reads them: the list's i atoms
+// (shifted by the exact lattice translation) and the current j tile, each as
+// four rows (x, y, z, q) of 32 doubles. A queued pair reads one double per
+// row per atom: the i reads of a step are mostly broadcasts (lane-major queue
+// order), the j reads span at most the 256 bytes of a row.
+struct Atoms64 {
+  double i[4][kWarp];
+  double j[4][kWarp];
+};
+
 // One lane's precise-pass sums over the current tile group.
 struct LaneSums {
   double eE, eS, w0, w1, w2, w3, w4, w5;
@@ -122,7 +127,11 @@ __device__ __forceinline__ double2 slowPair(const SlowTable& T, const unsigned k
 // The FP64 terms of one interacting pair (qq = 0 contributes exact zeros):
 // the fast energy qq (1/r - h(s)) with 1/r from the FP64 approximation
 // refined by one Newton step, and from the slow-term table the slow energy
-// qq phi_s(s) and the slow virial -2 qq phi_s'(s) d (x) d.
+// qq phi_s(s) and the slow virial -2 qq phi_s'(s) d (x) d. The geometry is
+// FP64 throughout: the electrostatic totals are small differences of large
+// sums (for 9,000 water atoms the fast energy is 4e-5 of the sum of its pair
+// terms' magnitudes), so even the unbiased FP32 rounding of r^2 would move
+// them by ~3e-6.
 template <bool doEnergy, bool doVirial, bool doSlow, int kCopies>
 __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable& T,
                                             const NbkConst& c, const int lane, LaneSums& L) {
@@ -173,39 +182,33 @@ __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable&
   }
 }
 
-// Queue entry e of the precise pass as FP64 pair terms; every lane takes
-// part in the shuffles. An entry past the end (e >= total) repeats entry 0, a
-// real pair (its atoms are distinct, so its distance is not 0), with qq = 0,
-// which contributes exact zeros.
+// Queue entry e of the precise pass as FP64 pair terms, from the warp's
+// atoms in shared memory. An entry past the end (e >= total) repeats entry 0,
+// a real pair (its atoms are distinct, so its distance is not 0), with
+// qq = 0, which contributes exact zeros.
 __device__ __forceinline__ void loadPair(const unsigned short* q, const int e, const int total,
-                                         const double4 ai, const double4 aj, PairTerms& u) {
+                                         const Atoms64& A, PairTerms& u) {
   const bool valid = e < total;
   const unsigned ent = q[valid ? e : 0];
   const int i = ent & 31, j = (i + (ent >> 5)) & 31;
-  const double ax = __shfl_sync(0xffffffffu, ai.x, i), ay = __shfl_sync(0xffffffffu, ai.y, i),
-               az = __shfl_sync(0xffffffffu, ai.z, i), aq = __shfl_sync(0xffffffffu, ai.w, i);
-  const double bx = __shfl_sync(0xffffffffu, aj.x, j), by = __shfl_sync(0xffffffffu, aj.y, j),
-               bz = __shfl_sync(0xffffffffu, aj.z, j), bq = __shfl_sync(0xffffffffu, aj.w, j);
-  u.dx = bx - ax;
-  u.dy = by - ay;
-  u.dz = bz - az;
-  u.qq = valid ? aq * bq : 0.0;
+  u.dx = A.j[0][j] - A.i[0][i];
+  u.dy = A.j[1][j] - A.i[1][i];
+  u.dz = A.j[2][j] - A.i[2][i];
+  u.qq = valid ? A.i[3][i] * A.j[3][j] : 0.0;
 }
 
 // The precise pass of one tile. live (per lane): bit t set when the pair
 // (i = lane, j = (lane + t) & 31) is an interacting pair (mask bit set and
 // FP32 r^2 below the cutoff, the classification the FP32 math used). The
 // warp compacts the tile's interacting pairs into a queue in shared memory
-// (entry = i | t << 5, lane-major order; at most 32 * 32 two-byte entries,
-// the 2 KB of pq) and processes them in FP64, two per lane per iteration
+// (entry = i | t << 5, lane-major order; at most 32 * 32 two-byte entries)
+// and processes them in FP64, two per lane per iteration
 // (entries e and e + 32: independent dependency chains) while more than 32
-// remain, then one. Lane l holds atom l of the list's i tile (ai: the FP64
-// shifted position and charge) and of the current j tile (aj, FP64), and a
-// pair's atoms come by shuffles (loadPair). Every step is warp-synchronous
-// and the sums depend only on the tile group.
+// remain, then one. A pair's atoms come from the warp's FP64 rows (loadPair).
+// Every step is warp-synchronous and the sums depend only on the tile group.
 template <bool doEnergy, bool doVirial, bool doSlow, int kCopies>
-__device__ __forceinline__ void precisePass(const unsigned live, const int lane, const double4 ai,
-                                            const double4 aj, double* pq, const SlowTable& T,
+__device__ __forceinline__ void precisePass(const unsigned live, const int lane, const Atoms64& A,
+                                            unsigned short* q, const SlowTable& T,
                                             const NbkConst& c, LaneSums& L, int& npair) {
   const int n = __popc(live);
   if (doEnergy) npair += n;
@@ -217,7 +220,6 @@ __device__ __forceinline__ void precisePass(const unsigned live, const int lane,
   }
   const int total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
   if (total == 0) return;  // warp-uniform
-  unsigned short* q = reinterpret_cast<unsigned short*>(pq);
   int pos = incl - n;
   // two set bits per iteration (the loop runs up to popc(live) / 2 times)
   for (unsigned w = live; w;) {
@@ -237,43 +239,54 @@ __device__ __forceinline__ void precisePass(const unsigned live, const int lane,
   for (; total - base > kWarp; base += 2 * kWarp) {  // warp-uniform
     PairTerms u[2];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) loadPair(q, base + h * kWarp + lane, total, ai, aj, u[h]);
+    for (int h = 0; h < 2; ++h) loadPair(q, base + h * kWarp + lane, total, A, u[h]);
 #pragma unroll
     for (int h = 0; h < 2; ++h) precisePair<doEnergy, doVirial, doSlow, kCopies>(u[h], T, c, lane, L);
   }
   if (base < total) {  // warp-uniform
     PairTerms u;
-    loadPair(q, base + lane, total, ai, aj, u);
+    loadPair(q, base + lane, total, A, u);
     precisePair<doEnergy, doVirial, doSlow, kCopies>(u, T, c, lane, L);
   }
-  __syncwarp();  // the queue is consumed before pq is written again
+  __syncwarp();  // the queue and the j rows are consumed before they are written again
 }
 
-// End of a tile group: each lane's sums are written to shared memory (pq,
-// [kNumQ][32]) and reduced per quantity in a fixed order (lane L sums
-// quantity L & 7 over lanes 8 (L >> 3) .. 8 (L >> 3) + 7, then two butterfly
-// steps combine the four groups), and lane q < kNumQ adds quantity q, in
-// fixed point, to accQ; the sums restart at zero.
-__device__ __forceinline__ void reduceGroup(const int lane, double* pq, LaneSums& L,
-                                            long long& accQ) {
-  pq[kQElec * kWarp + lane] = L.eE;
-  pq[kQSlow * kWarp + lane] = L.eS;
-  pq[(kQVir + 0) * kWarp + lane] = L.w0;
-  pq[(kQVir + 1) * kWarp + lane] = L.w1;
-  pq[(kQVir + 2) * kWarp + lane] = L.w2;
-  pq[(kQVir + 3) * kWarp + lane] = L.w3;
-  pq[(kQVir + 4) * kWarp + lane] = L.w4;
-  pq[(kQVir + 5) * kWarp + lane] = L.w5;
-  __syncwarp();
-  const double* src = pq + (lane & 7) * kWarp + (lane >> 3) * 8;
-  double v = src[0];
+// End of a tile group: the lanes' sums are reduced per quantity by a fixed
+// butterfly that halves the quantities a lane holds at each step (lanes l and
+// l ^ 16 exchange four of their eight, then l ^ 8 two, l ^ 4 one; two more
+// steps add within groups of four lanes), so that lane 4q holds the warp's
+// total of quantity q; lane q < kNumQ then adds quantity q, in fixed point,
+// to accQ, and the sums restart at zero. No shared memory: a transposition
+// through it costs more than these 20 shuffles (its reads conflict 16-way).
+__device__ __forceinline__ void reduceGroup(const int lane, LaneSums& L, long long& accQ) {
+  double v[kNumQ] = {L.eE, L.eS, L.w0, L.w1, L.w2, L.w3, L.w4, L.w5};
+  static_assert(kQElec == 0 && kQSlow == 1 && kQVir == 2 && kNumQ == 8, "quantity order");
+  // lanes with bit 4 set keep quantities 4..7, the others 0..3
+  const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
 #pragma unroll
-  for (int m = 1; m < 8; ++m) v += src[m];
-  v += __shfl_xor_sync(0xffffffffu, v, 8);
-  v += __shfl_xor_sync(0xffffffffu, v, 16);
-  if (lane < kNumQ) accQ += toFixedEnergy(v);
+  for (int k = 0; k < 4; ++k) {
+    const double send = b4 ? v[k] : v[k + 4];
+    const double keep = b4 ? v[k + 4] : v[k];
+    v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const double send = b3 ? v[k] : v[k + 2];
+    const double keep = b3 ? v[k + 2] : v[k];
+    v[k] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+  {
+    const double send = b2 ? v[0] : v[1];
+    const double keep = b2 ? v[1] : v[0];
+    v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  // lane l now holds quantity (l >> 2) summed over the lanes l' with
+  // l' & 3 == l & 3; complete the sums within each group of four lanes
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+  v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+  const double tot = __shfl_sync(0xffffffffu, v[0], 4 * (lane & 7));
+  if (lane < kNumQ) accQ += toFixedEnergy(tot);
   L = LaneSums{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-  __syncwarp();  // pq is free for the next tile's queue
 }
 
 // MINB: CTAs per SM the register budget is cut for (4, 5 or 6 -> 128, 96 or
@@ -556,22 +569,25 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
 }
 
 // The precise kernel: one warp per refined tile list (handed out by a global
-// counter in the force kernel's order, longest first). Per list the FP64
-// shifted i atoms go to shared memory (the shift formed in FP64 from the FP32
-// offsets and lattice: the exact lattice translation, without the FP32
-// rounding of the force kernel's shift); per tile with interacting pairs the
-// j atoms (FP32) and the precise pass; per group of kFoldTiles tiles (counted
-// from the list start, as the force kernel's) the lanes' sums go into fixed
-// point. Results do not depend on the order in which lists run.
+// counter in the force kernel's order, longest first). Per list the i atoms,
+// shifted in FP64 by the shift formed in FP64 from the FP32 offsets and
+// lattice (the exact lattice translation, without the FP32 rounding of the
+// force kernel's shift), go to the warp's FP64 rows; per tile with interacting
+// pairs the j atoms and the precise pass; per group of kFoldTiles tiles
+// (counted from the list start, as the force kernel's) the lanes' sums go into
+// fixed point. Results do not depend on the order in which lists run.
 constexpr int kPreciseWarps = 8;
 constexpr int kPreciseThreads = kPreciseWarps * kWarp;
+constexpr int kPreciseMinBlocks = 3;
 
 template <bool doEnergy, bool doVirial, bool doSlow, bool doBatch, int kCopies>
-__global__ void __launch_bounds__(kPreciseThreads, 3)
+__global__ void __launch_bounds__(kPreciseThreads, kPreciseMinBlocks)
     preciseKernel(const __grid_constant__ ForceArgs a) {
-  __shared__ double s_pq[kPreciseWarps][kNumQ * kWarp];
+  __shared__ unsigned short s_queue[kPreciseWarps][kWarp * kWarp];
+  __shared__ Atoms64 s_atoms[kPreciseWarps];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
+  Atoms64& A = s_atoms[wib];
   SlowTable T;
   T.last = (unsigned)(a.slowTableRows - 1);
   T.step = a.slowStep;
@@ -608,17 +624,13 @@ __global__ void __launch_bounds__(kPreciseThreads, 3)
       lb = a.repLat[3 * rep + 1];
       lc = a.repLat[3 * rep + 2];
     }
-    // this lane's i atom, shifted in FP64 by the shift formed in FP64 from the
-    // FP32 offsets and lattice (the exact lattice translation, without the
-    // FP32 rounding of the force kernel's shift)
-    const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
-    double4 ai;
     {
+      const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
       const float4 xi = a.xyzq[tl.iatomStart + lane];
-      ai.x = (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x);
-      ai.y = (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y);
-      ai.z = (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z);
-      ai.w = (double)xi.w;
+      A.i[0][lane] = (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x);
+      A.i[1][lane] = (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y);
+      A.i[2][lane] = (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z);
+      A.i[3][lane] = (double)xi.w;
     }
     // the next tile's live word and j atom are loaded while the current tile
     // is processed; the j-tile starts come 32 at a time (lane t holds tile
@@ -641,12 +653,16 @@ __global__ void __launch_bounds__(kPreciseThreads, 3)
         xjNext = a.xyzq[__shfl_sync(0xffffffffu, jsBlock, t + 1) + lane];
       }
       if (__any_sync(0xffffffffu, live != 0u)) {
-        const double4 aj = make_double4((double)xj.x, (double)xj.y, (double)xj.z, (double)xj.w);
-        precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, ai, aj, s_pq[wib], T, a.c,
+        // the i rows and this j tile are visible after the pass's first __syncwarp
+        A.j[0][lane] = (double)xj.x;
+        A.j[1][lane] = (double)xj.y;
+        A.j[2][lane] = (double)xj.z;
+        A.j[3][lane] = (double)xj.w;
+        precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, A, s_queue[wib], T, a.c,
                                                          lsum, npair);
       }
       if (((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0 || jt == tl.jtileEnd)
-        reduceGroup(lane, s_pq[wib], lsum, accQ);
+        reduceGroup(lane, lsum, accQ);
     }
   }
   flushPrecise<doEnergy>(a.acc + (size_t)curRep * kAccCount, lane, accQ, npair);
@@ -752,11 +768,11 @@ static cudaError_t launchPC(const ForceArgs& a, int numSM, cudaStream_t st) {
                           a);
 }
 
-// the table in shared memory with 8 interleaved copies when they fit in 32 KB
-// (64 rows), else read from global memory
+// the table in shared memory with 8 interleaved copies when they fit in 40 KB
+// (106 rows), else read from global memory
 template <bool E, bool V, bool S, bool B>
 static cudaError_t launchP(const ForceArgs& a, int numSM, cudaStream_t st) {
-  if (sizeof(double) * kSlowTableDeg1 * (size_t)a.slowTableRows * 8 <= 32 * 1024)
+  if (sizeof(double) * kSlowTableDeg1 * (size_t)a.slowTableRows * 8 <= 40 * 1024)
     return launchPC<E, V, S, B, 8>(a, numSM, st);
   return launchPC<E, V, S, B, 0>(a, numSM, st);
 }

@@ -48,11 +48,11 @@ struct NbkConst {
   float s0;           // 0 with switching, 1 without (packed math: S = d^2 P + s0)
   int ljDim;          // LJ table row length
   int switching;      // 0 when switchdist >= cutoff (plain truncated LJ)
-  double hAd, hBd;    // hA, hB in FP64 (FP64 energy mode)
+  double hAd, hBd;    // hA, hB in FP64 (precise kernel)
   double betad;       // Ewald coefficient in FP64
 };
 
-// FP64 copies of the pair-math constants (FP64 energy/virial mode).
+// FP64 copies of the pair-math constants (the corrections kernel's energies and slow virial).
 struct NbkConst64 {
   double rc2, rs2, lj0, lj1, lj2, lj3, rc3inv, hA, hB, beta, beta2Pi, one14;
   int switching;
@@ -162,7 +162,7 @@ __device__ __forceinline__ double rsqrtApprox64(double x) {
 //   slow    E = qq ((3 - r^2/rc^2)/(2 rc) + (erfc(beta r) - 1)/r)
 // (src/CudaComputeNonbondedInteractions.h:37-159 states the same forms.) Only
 // the LJ energy is summed here (doVdwEnergy): the electrostatic energies and
-// the slow virial are formed in FP64 by the force kernel's precise pass.
+// the slow virial are formed in FP64 by the precise kernel (nbk_force.cu).
 // An element with qq = A = nB = 0 and r2 = cutoff^2 contributes exactly zero
 // to F, FS and the energy, which is how callers switch a pair off without a
 // branch. The slow term regroups the same quantities: with x = beta r,
@@ -213,18 +213,21 @@ __device__ __forceinline__ void pairForce2(const float2 r2, const float2 qq, con
 // The slow electrostatic energy per unit qq, phi_s(s) = h(s) - erf(beta sqrt(s))/sqrt(s)
 // with s = r^2 and h(s) = (3 - s/rc^2)/(2 rc), is an entire function of s (the
 // 1/r singularities of erfc(beta r)/r and of the fast part cancel), so a
-// piecewise polynomial in s represents it to FP64 rounding: with a step D (a
-// power of two, at most 32 A^2), row k holds the degree-7 Chebyshev
-// interpolant on s in [k D - D/2, k D + D/2] in the monomial basis of
-// w = s - k D (8 coefficients, 64 bytes: four 16-byte loads per pair). Its
-// derivative gives the slow force factor, (dE/dr)/r = 2 qq phi_s'(s),
-// without the rc^-3 - r^-3 cancellation of the FP32 form. Built on the host at
-// handle creation (buildSlowTable) from FP64 erf, with D chosen so that the
-// fit is within FP64 rounding (48 rows at the benchmark's parameters).
+// piecewise polynomial in s represents it closely: with a step D (a power of
+// two, at most 32 A^2), row k holds the degree-5 Chebyshev interpolant on s in
+// [k D - D/2, k D + D/2] in the monomial basis of w = s - k D (6 coefficients,
+// 48 bytes: three 16-byte loads per pair). Its derivative gives the slow force
+// factor, (dE/dr)/r = 2 qq phi_s'(s), without the rc^-3 - r^-3 cancellation of
+// the FP32 form. Built on the host at handle creation (buildSlowTable) from
+// FP64 erf, with D chosen so that the fit is within 1e-12 of the function's
+// scale and its derivative within ~1e-9 (94 rows at the benchmark's
+// parameters): a systematic error that, even summed over every pair with the
+// same sign, stays below 1e-7 of the slow energy.
 constexpr double kSlowTableStepMax = 32.0;  // A^2
-constexpr int kSlowTableDeg = 7;
+constexpr int kSlowTableDeg = 5;
 constexpr int kSlowTableDeg1 = kSlowTableDeg + 1;  // coefficients per row
-constexpr int kSlowTableRow = 8;  // doubles per row of the global copy
+constexpr int kSlowTableRow = 6;  // doubles per row of the global copy
+constexpr double kSlowTableTol = 1e-12;  // fit error, relative to max |phi_s| + 1/rc
 
 // Component k (0..8, row-major 3x3) of a symmetric tensor stored as
 // xx, xy, xz, yy, yz, zz.

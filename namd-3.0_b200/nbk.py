@@ -646,16 +646,19 @@ class Nonbonded:
         return tl[:nl.value], ja[:nj.value], ex[:nj.value]
 
 
+SLOW_TABLE_ROW = 6  # doubles per row of nbk_slow_table (degree-5 polynomials)
+
+
 def slow_table(ewaldcof: float, cutoff: float, pairlistdist: float):
     """The FP64 slow-term table of the precise pass (nbk_slow_table): (rows,
-    step) where row k (8 doubles) holds c0..c7 of
+    step) where row k (SLOW_TABLE_ROW = 6 doubles) holds c0..c5 of
     phi_s(s) ~ sum c_n (s - k step)^n on s in [k step - step/2, k step + step/2];
     host-only."""
     L = dev_lib()
     rows = L.nbk_slow_table(ewaldcof, cutoff, pairlistdist, None, 0, None)
     if rows <= 0:
         raise NbkError(f"nbk_slow_table failed ({rows})")
-    out = np.zeros((rows, 8))
+    out = np.zeros((rows, SLOW_TABLE_ROW))
     step = C.c_double(0.0)
     rc = L.nbk_slow_table(ewaldcof, cutoff, pairlistdist, out.ctypes.data, rows, C.byref(step))
     if rc != rows:

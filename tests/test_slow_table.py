@@ -11,7 +11,7 @@ import nbk
 from helpers import PARAMS
 
 
-DEG = 7    # polynomial degree of a row (8 coefficients)
+DEG = 5    # polynomial degree of a row (6 coefficients)
 
 
 def _eval(T, step, s):
@@ -33,7 +33,7 @@ def _eval(T, step, s):
                                             (0.6, 6.0, 7.5)])
 def test_slow_table_matches_the_slow_term(beta, cutoff, pl):
     T, step = nbk.slow_table(beta, cutoff, pl)
-    assert T.shape[1] == 8
+    assert T.shape[1] == DEG + 1
     assert step <= 32.0 and math.log2(step) == round(math.log2(step))
     # rows cover s up to pairlistdist^2 + 2
     assert step * (T.shape[0] - 1) + step / 2 >= pl * pl + 2
@@ -48,9 +48,10 @@ def test_slow_table_matches_the_slow_term(beta, cutoff, pl):
     g = (-1.0 / rc ** 3 + erf(beta * r) / r ** 3
          - 2.0 * beta / math.sqrt(math.pi) * np.exp(-beta * beta * s) / s)
     p, dp = _eval(T, step, s)
-    assert np.abs(p - phi).max() <= 2e-14 * np.abs(phi).max()
-    # per pair, a slow virial term g r^2 is then off by < 3e-10 per unit qq
-    assert np.abs(2.0 * dp - g).max() <= 2e-11 * np.abs(g).max()
+    # the builder's bound: 1e-12 of max |phi_s| + 1/rc
+    assert np.abs(p - phi).max() <= 1e-12 * (np.abs(phi).max() + 1.0 / rc)
+    # the derivative, one order less smooth, within 2e-9 of the largest factor
+    assert np.abs(2.0 * dp - g).max() <= 2e-9 * np.abs(g).max()
 
 
 def test_slow_table_rejects_bad_parameters():
@@ -58,5 +59,5 @@ def test_slow_table_rejects_bad_parameters():
     assert L.nbk_slow_table(0.26, -1.0, 13.5, None, 0, None) < 0
     assert L.nbk_slow_table(0.26, 12.0, 11.0, None, 0, None) < 0
     rows = L.nbk_slow_table(0.26, 12.0, 13.5, None, 0, None)
-    out = np.zeros((rows - 1, 8))
+    out = np.zeros((rows - 1, DEG + 1))
     assert L.nbk_slow_table(0.26, 12.0, 13.5, out.ctypes.data, rows - 1, None) < 0
