@@ -174,6 +174,11 @@ struct nbk_context {
   bool timing = false;
   std::vector<cudaEvent_t> evStart, evMid, evStop;
   int numTimed = 0;
+  // second stream for the work that does not wait for the precise kernel
+  // (corrections, force finalize, output copies), forked from and joined
+  // back into the caller's stream within each evaluation
+  cudaStream_t side = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
 };
 
 namespace {
@@ -196,6 +201,21 @@ cudaError_t timedEvent(nbk_context* h, TimedPoint which, cudaStream_t st) {
   }
   cudaError_t r = cudaEventRecord(v[k], st);
   if (which == kTimedStop) ++h->numTimed;
+  return r;
+}
+
+// The handle's side stream and its fork / join events, made on first use.
+cudaError_t ensureSideStream(nbk_context* h) {
+  if (h->side) return cudaSuccess;
+  cudaError_t r = cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming);
+  if (r == cudaSuccess) r = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+  if (r != cudaSuccess) {
+    if (h->evFork) cudaEventDestroy(h->evFork);
+    if (h->evJoin) cudaEventDestroy(h->evJoin);
+    h->evFork = h->evJoin = nullptr;
+    h->side = nullptr;
+  }
   return r;
 }
 }  // namespace
@@ -409,7 +429,13 @@ NBK_API int nbk_destroy(nbk_handle h) {
   h->repLJ.release();
   h->repLJExcl.release();
   for (cudaEvent_t e : h->evStart) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->evMid) cudaEventDestroy(e);
   for (cudaEvent_t e : h->evStop) cudaEventDestroy(e);
+  if (h->side) {
+    cudaStreamDestroy(h->side);
+    cudaEventDestroy(h->evFork);
+    cudaEventDestroy(h->evJoin);
+  }
   delete h;
   return NBK_OK;
 }
@@ -690,16 +716,28 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
   NBK_CUDA(launchForce(a, flags, h->tuneMinBlocks[key], h->numSM, st), "force kernel");
   h->launches += 1;
   NBK_CUDA(timedEvent(h, kTimedMid, st), "timing event");
-  if (needsPrecise(flags)) {
+  const bool corrections = (flags & NBK_CORRECTIONS) && (h->numMod || h->numExc);
+  if (corrections && h->maxTupleSlot >= n)
+    return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: a correction tuple names a slot beyond atomStorageSize");
+  if ((h_forces && !d_forces) || (h_forcesSlow && !d_forcesSlow))
+    return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: host force output needs the matching device buffer");
+  // With a precise kernel to run, the corrections, the force finalize and the
+  // output copies (which need only the forces) go to the side stream and run
+  // beside it; the caller's stream waits for both before it goes on.
+  const bool fork = needsPrecise(flags);
+  cudaStream_t fs = st;
+  if (fork) {
+    NBK_CUDA(ensureSideStream(h), "nbk_nonbonded_force: side stream");
+    NBK_CUDA(cudaEventRecord(h->evFork, st), "nbk_nonbonded_force: fork");
+    NBK_CUDA(cudaStreamWaitEvent(h->side, h->evFork, 0), "nbk_nonbonded_force: fork");
+    fs = h->side;
     ForceArgs pa = a;
     pa.workCounter = h->counters.p + 4;
     NBK_CUDA(launchPrecise(pa, flags, h->numSM, st), "precise energy / virial kernel");
     h->launches += 1;
   }
   NBK_CUDA(timedEvent(h, kTimedStop, st), "timing event");
-  if ((flags & NBK_CORRECTIONS) && (h->numMod || h->numExc)) {
-    if (h->maxTupleSlot >= n)
-      return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: a correction tuple names a slot beyond atomStorageSize");
+  if (corrections) {
     CorrArgs ca{};
     ca.modified = h->modTuples.p;
     ca.numModified = h->numMod;
@@ -721,7 +759,7 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
       ca.repLat = h->repLat.p;
       ca.repLJExcl = h->repLJExcl.p;
     }
-    NBK_CUDA(launchCorrections(ca, flags, st), "exclusion corrections");
+    NBK_CUDA(launchCorrections(ca, flags, fs), "exclusion corrections");
     h->launches += 1;
   }
   ShiftVirialArgs sv{};
@@ -735,27 +773,29 @@ NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flag
     sv.compRep = h->nrep ? h->compRep.p : nullptr;
     sv.repLat = h->nrep ? h->repLat.p : nullptr;
   }
-  if ((h_forces && !d_forces) || (h_forcesSlow && !d_forcesSlow))
-    return setErr(NBK_ERR_ARG, "nbk_nonbonded_force: host force output needs the matching device buffer");
   // page-locked host outputs are written by the finalize kernel itself;
   // other host memory gets a copy after it
   float4* hF = static_cast<float4*>(mappedHostPointer(h_forces));
   float4* hS = (flags & NBK_SLOW) ? static_cast<float4*>(mappedHostPointer(h_forcesSlow)) : nullptr;
   NBK_CUDA(launchFinalizeForces(n, h->force.p, n, h->xyzq, reinterpret_cast<float4*>(d_forces),
                                 (flags & NBK_SLOW) ? reinterpret_cast<float4*>(d_forcesSlow) : nullptr,
-                                flags, h->acc.p, h->numSM, st, h->nrep ? h->slotRep.p : nullptr,
+                                flags, h->acc.p, h->numSM, fs, h->nrep ? h->slotRep.p : nullptr,
                                 &sv, hF, hS),
            "force finalize");
   if ((flags & NBK_VIRIAL) || d_forces || d_forcesSlow) h->launches += 1;
   if (d_forcesFixed)
     NBK_CUDA(cudaMemcpyAsync(d_forcesFixed, h->force.p, sizeof(long long) * 6 * (size_t)n,
-                             cudaMemcpyDeviceToDevice, st), "nbk_nonbonded_force: fixed-point copy");
+                             cudaMemcpyDeviceToDevice, fs), "nbk_nonbonded_force: fixed-point copy");
   if (h_forces && !hF)
-    NBK_CUDA(cudaMemcpyAsync(h_forces, d_forces, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, st),
+    NBK_CUDA(cudaMemcpyAsync(h_forces, d_forces, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToHost, fs),
              "nbk_nonbonded_force: D2H");
   if (h_forcesSlow && (flags & NBK_SLOW) && !hS)
     NBK_CUDA(cudaMemcpyAsync(h_forcesSlow, d_forcesSlow, sizeof(float4) * (size_t)n,
-                             cudaMemcpyDeviceToHost, st), "nbk_nonbonded_force: D2H");
+                             cudaMemcpyDeviceToHost, fs), "nbk_nonbonded_force: D2H");
+  if (fork) {
+    NBK_CUDA(cudaEventRecord(h->evJoin, fs), "nbk_nonbonded_force: join");
+    NBK_CUDA(cudaStreamWaitEvent(st, h->evJoin, 0), "nbk_nonbonded_force: join");
+  }
   h->lastFlags = flags;
   return NBK_OK;
 }
