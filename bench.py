@@ -367,14 +367,17 @@ class _DeviceArray:
                                          "data": (int(ptr), False), "version": 3}
 
 
-def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, value, flush):
+def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, value, flush,
+                       do_table=1, slow=1, max_steps=500):
     """The reference's plain GPU path (its own tile-list and nonbonded kernels,
-    built from the reference tree into oracle/_ref; texture-table mode, its
-    choice whenever slow forces are on) on the same trajectory and protocol as
-    the timed region: force + energy + virial + slow every step, lists rebuilt
-    every REBUILD steps. Steady steps copy the frame on the device into the
-    reference's position buffer; pairlist steps hand it the page-locked host
-    frame, as its tile-list build takes positions from the host. The same
+    built from the reference tree into oracle/_ref) on the same trajectory and
+    protocol as the timed region: lists rebuilt every REBUILD steps. With
+    do_table=1, slow=1: texture-table mode (its choice whenever slow forces
+    are on), force + energy + virial + slow every step, the timed region's
+    flags. With do_table=0, slow=0: its direct-math mode (force + energy +
+    virial, no slow forces). Steady steps copy the frame on the device into
+    the reference's position buffer; pairlist steps hand it the page-locked
+    host frame, as its tile-list build takes positions from the host. The same
     GPU-counted pairs per frame give its pairs/s. None when the harness is not
     built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -385,7 +388,8 @@ def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, va
     import nbk
     dev = torch.device("cuda", local_rank)
     n = packed.atomStorageSize
-    ref = refgpu.RefGpu(nbk.NonbondedParams(), sys_.lj_table(), do_table=1, device=local_rank)
+    ref = refgpu.RefGpu(nbk.NonbondedParams(), sys_.lj_table(), do_table=do_table,
+                        device=local_rank)
     ref.setup(packed)
     rs = torch.cuda.ExternalStream(ref.stream_ptr)
     state = {}
@@ -393,7 +397,7 @@ def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, va
     def step(k):
         f = k % NFRAMES
         if k % REBUILD == 0:
-            ref.eval(1, 1, 1, 1, pin[f].numpy())
+            ref.eval(1, 1, 1, slow, pin[f].numpy())
             ptr = refgpu.lib().refgpu_device_xyzq(ref._h)
             if state.get("ptr") != ptr:
                 state["ptr"] = ptr
@@ -401,12 +405,12 @@ def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, va
         else:
             with torch.cuda.stream(rs):
                 state["view"].copy_(frames[f])
-            ref.eval(0, 1, 1, 1, None)
+            ref.eval(0, 1, 1, slow, None)
 
     for k in range(max(args.warmup, 3)):
         step(k)
     ref.sync()
-    ksteps = min(args.steps, 500)
+    ksteps = min(args.steps, max_steps)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(ksteps)]
     for k in range(ksteps):
@@ -422,7 +426,9 @@ def reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank, va
     out = {"value": v, "unit": UNIT, "steps": ksteps, "ms_per_step": float(ms.mean()),
            "steady_ms": float(np.mean([ms[k] for k in range(ksteps) if k % REBUILD])),
            "pairlist_ms": float(np.mean([ms[k] for k in range(ksteps) if k % REBUILD == 0])),
-           "mode": "reference CudaTileListKernel + CudaComputeNonbondedKernel, texture tables",
+           "mode": ("reference CudaTileListKernel + CudaComputeNonbondedKernel, " +
+                    ("texture tables, force + energy + virial + slow" if do_table else
+                     "direct math, force + energy + virial (no slow forces)")),
            "product_over_reference": value / v}
     del ref
     return out
@@ -627,6 +633,43 @@ def run_gpu(args, rank, world, local_rank):
     if rank == 0 and world == 1:
         plain_gpu = reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank,
                                        value, flush)
+        if plain_gpu is not None:
+            # the reference's direct-math mode (no slow forces) against the
+            # product with the same flags, same protocol
+            fl_ev = nbk.NBK_ENERGY | nbk.NBK_VIRIAL
+            kev = min(args.steps, 200)
+
+            def step_ev(k):
+                f = k % NFRAMES
+                x = frames[f]
+                if k % REBUILD == 0:
+                    nb.build_tile_lists(packed, xyzq=x, stream=st)
+                    nb.force(packed, fl_ev | nbk.NBK_PAIRLIST, xyzq=x, d_forces=dF, stream=st)
+                else:
+                    nb.force(packed, fl_ev, xyzq=x, d_forces=dF, stream=st)
+                nb.virial_energy_to(dVE.data_ptr(), True, fl_ev, stream=st)
+
+            for k in range(args.warmup):
+                step_ev(k)
+            evv = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                   for _ in range(kev)]
+            for k in range(kev):
+                flush.zero_()
+                evv[k][0].record(stream)
+                step_ev(k)
+                evv[k][1].record(stream)
+            torch.cuda.synchronize(dev)
+            ms_ev = np.array([a.elapsed_time(b) for a, b in evv])
+            v_ev = sum(pairs_of[k % NFRAMES] for k in range(kev)) / (ms_ev.sum() * 1e-3)
+            ref_ev = reference_protocol(sys_, packed, frames, pin, pairs_of, args, local_rank,
+                                        v_ev, flush, do_table=0, slow=0, max_steps=200)
+            plain_gpu["energy_virial_direct_math"] = {
+                "product": {"value": float(v_ev), "unit": UNIT, "steps": kev,
+                            "ms_per_step": float(ms_ev.mean()),
+                            "steady_ms": float(np.mean([ms_ev[k] for k in range(kev) if k % REBUILD])),
+                            "pairlist_ms": float(np.mean([ms_ev[k] for k in range(kev)
+                                                          if k % REBUILD == 0]))},
+                "reference": ref_ev}
     build_t = tile_build_timing(nb, packed, frames[0], stream)
     nb.force(packed, FL | nbk.NBK_PAIRLIST, xyzq=frames[0], d_forces=dF, d_forcesSlow=dS,
              stream=st)
@@ -906,6 +949,32 @@ def run_adjoint(args, rank, world, local_rank):
         "config": {"workload": out["workload"]}, "adjoint": out}))
 
 
+def run_profile_case(args, local_rank):
+    """The short fixed launch sequence that kernel captures run under ncu: the
+    workload's system (seed 2), one tile-list build and pairlist evaluation,
+    then three steady E+V+S evaluations at launch shape (5, 1) with kernel
+    timing on. Prints the force and precise kernel times; no JSON line."""
+    import torch
+    import nbk
+    torch.cuda.set_device(local_rank)
+    fl = nbk.NBK_ENERGY | nbk.NBK_VIRIAL | nbk.NBK_SLOW
+    sys_ = nbk.System(nbk.NBK_SYS_MIXED, 2, NATOMS, FRAC, box=BOX)
+    packed = nbk.Packed(sys_)
+    nb = nbk.Nonbonded(nbk.NonbondedParams(), sys_.lj_table(), local_rank)
+    nb.setup(packed)
+    x = torch.from_numpy(packed.xyzq.copy()).cuda()
+    nb.build_tile_lists(packed, xyzq=x)
+    nb.force(packed, fl | nbk.NBK_PAIRLIST, xyzq=x)
+    nb.set_tuning(fl, 5, 1)
+    nb.set_kernel_timing(True)
+    for _ in range(3):
+        nb.force(packed, fl, xyzq=x)
+    torch.cuda.synchronize()
+    log("profile case: force kernel ms", list(nb.kernel_times()), "precise kernel ms",
+        list(nb.precise_times()))
+    nb.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -920,6 +989,9 @@ def main():
                     default="mixed92k",
                     help="batch64: 64-replica batched launch vs one launch per replica; "
                          "large1m: the 1,066,628-atom system of the precision study")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="run only the short launch sequence that ncu kernel captures use "
+                         "(one pairlist and three steady evaluations of the workload's system)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -928,6 +1000,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "large1m":
         use_large_system()
+    if args.profile_case:
+        run_profile_case(args, local_rank)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
