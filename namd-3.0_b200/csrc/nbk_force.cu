@@ -87,12 +87,12 @@ struct PairTerms {
 
 // The warp's atoms in FP64 as the precise pass reads them: the list's i atoms
 // (shifted by the exact lattice translation) and the current j tile, each as
-// four rows (x, y, z, q) of 32 doubles. A queued pair reads one double per
-// row per atom: the i reads of a step are mostly broadcasts (lane-major queue
-// order), the j reads span at most the 256 bytes of a row.
+// two rows of 32 (x, y) and (z, q) pairs. A queued pair reads two 16-byte
+// entries per atom: the i reads of a step are mostly broadcasts (lane-major
+// queue order), the j reads span at most the 512 bytes of a row.
 struct Atoms64 {
-  double i[4][kWarp];
-  double j[4][kWarp];
+  double2 ixy[kWarp], izq[kWarp];
+  double2 jxy[kWarp], jzq[kWarp];
 };
 
 // One lane's precise-pass sums over the current tile group.
@@ -191,10 +191,11 @@ __device__ __forceinline__ void loadPair(const unsigned short* q, const int e, c
   const bool valid = e < total;
   const unsigned ent = q[valid ? e : 0];
   const int i = ent & 31, j = (i + (ent >> 5)) & 31;
-  u.dx = A.j[0][j] - A.i[0][i];
-  u.dy = A.j[1][j] - A.i[1][i];
-  u.dz = A.j[2][j] - A.i[2][i];
-  u.qq = valid ? A.i[3][i] * A.j[3][j] : 0.0;
+  const double2 ia = A.ixy[i], ib = A.izq[i], ja = A.jxy[j], jb = A.jzq[j];
+  u.dx = ja.x - ia.x;
+  u.dy = ja.y - ia.y;
+  u.dz = jb.x - ib.x;
+  u.qq = valid ? ib.y * jb.y : 0.0;
 }
 
 // The precise pass of one tile. live (per lane): bit t set when the pair
@@ -627,10 +628,12 @@ __global__ void __launch_bounds__(kPreciseThreads, kPreciseMinBlocks)
     {
       const float3 off = make_float3(tl.offsetXYZ.x, tl.offsetXYZ.y, tl.offsetXYZ.z);
       const float4 xi = a.xyzq[tl.iatomStart + lane];
-      A.i[0][lane] = (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x);
-      A.i[1][lane] = (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y);
-      A.i[2][lane] = (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z);
-      A.i[3][lane] = (double)xi.w;
+      A.ixy[lane] = make_double2(
+          (double)xi.x + ((double)off.x * la.x + (double)off.y * lb.x + (double)off.z * lc.x),
+          (double)xi.y + ((double)off.x * la.y + (double)off.y * lb.y + (double)off.z * lc.y));
+      A.izq[lane] = make_double2(
+          (double)xi.z + ((double)off.x * la.z + (double)off.y * lb.z + (double)off.z * lc.z),
+          (double)xi.w);
     }
     // the next tile's live word and j atom are loaded while the current tile
     // is processed; the j-tile starts come 32 at a time (lane t holds tile
@@ -654,10 +657,8 @@ __global__ void __launch_bounds__(kPreciseThreads, kPreciseMinBlocks)
       }
       if (__any_sync(0xffffffffu, live != 0u)) {
         // the i rows and this j tile are visible after the pass's first __syncwarp
-        A.j[0][lane] = (double)xj.x;
-        A.j[1][lane] = (double)xj.y;
-        A.j[2][lane] = (double)xj.z;
-        A.j[3][lane] = (double)xj.w;
+        A.jxy[lane] = make_double2((double)xj.x, (double)xj.y);
+        A.jzq[lane] = make_double2((double)xj.z, (double)xj.w);
         precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, A, s_queue[wib], T, a.c,
                                                          lsum, npair);
       }
