@@ -85,14 +85,16 @@ struct PairTerms {
   double dx, dy, dz, qq;
 };
 
-// The warp's atoms in FP64 as the precise pass reads them: the list's i atoms
-// (shifted by the exact lattice translation) and the current j tile, each as
-// two rows of 32 (x, y) and (z, q) pairs. A queued pair reads two 16-byte
-// entries per atom: the i reads of a step are mostly broadcasts (lane-major
-// queue order), the j reads span at most the 512 bytes of a row.
+// The warp's atoms as the precise pass reads them: the list's i atoms in FP64
+// (shifted by the exact lattice translation) as two rows of 32 (x, y) and
+// (z, q) pairs, and the current j tile as it is stored (FP32 x, y, z, q, exact
+// in FP64). A queued pair reads two 16-byte entries of its i atom, mostly
+// broadcasts (lane-major queue order), and one of its j atom: the j reads
+// span the 512 bytes of the row, half of what FP64 rows would, and the four
+// conversions to FP64 cost less than the second load.
 struct Atoms64 {
   double2 ixy[kWarp], izq[kWarp];
-  double2 jxy[kWarp], jzq[kWarp];
+  float4 j[kWarp];
 };
 
 // One lane's precise-pass sums over the current tile group.
@@ -191,11 +193,12 @@ __device__ __forceinline__ void loadPair(const unsigned short* q, const int e, c
   const bool valid = e < total;
   const unsigned ent = q[valid ? e : 0];
   const int i = ent & 31, j = (i + (ent >> 5)) & 31;
-  const double2 ia = A.ixy[i], ib = A.izq[i], ja = A.jxy[j], jb = A.jzq[j];
-  u.dx = ja.x - ia.x;
-  u.dy = ja.y - ia.y;
-  u.dz = jb.x - ib.x;
-  u.qq = valid ? ib.y * jb.y : 0.0;
+  const double2 ia = A.ixy[i], ib = A.izq[i];
+  const float4 jb = A.j[j];
+  u.dx = (double)jb.x - ia.x;
+  u.dy = (double)jb.y - ia.y;
+  u.dz = (double)jb.z - ib.x;
+  u.qq = valid ? ib.y * (double)jb.w : 0.0;
 }
 
 // The precise pass of one tile. live (per lane): bit t set when the pair
@@ -657,8 +660,7 @@ __global__ void __launch_bounds__(kPreciseThreads, kPreciseMinBlocks)
       }
       if (__any_sync(0xffffffffu, live != 0u)) {
         // the i rows and this j tile are visible after the pass's first __syncwarp
-        A.jxy[lane] = make_double2((double)xj.x, (double)xj.y);
-        A.jzq[lane] = make_double2((double)xj.z, (double)xj.w);
+        A.j[lane] = xj;
         precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, A, s_queue[wib], T, a.c,
                                                          lsum, npair);
       }
