@@ -74,6 +74,40 @@ def test_forces_mixed(mixed, corr):
     _check_forces(mixed, corr)
 
 
+@pytest.mark.parametrize("beta,cutoff,switch,pl", [(0.34, 10.0, 8.5, 11.5), (0.43, 8.0, 7.0, 9.5)])
+def test_forces_other_cutoffs(mixed, beta, cutoff, switch, pl):
+    """Shorter cutoffs with the Ewald coefficients that a PME tolerance of
+    1e-6 gives for them, against the oracle with the same parameters: the
+    pair set, forces, energies and virials. With these the precise kernel's
+    slow-term table (136 and 186 rows) is too large for shared memory and is
+    read from global memory."""
+    import dataclasses
+    s, p, _ = mixed
+    params = dataclasses.replace(PARAMS, ewaldcof=beta, cutoff=cutoff, switchdist=switch,
+                                 pairlistdist=pl)
+    T, _ = nbk.slow_table(beta, cutoff, pl)
+    assert T.shape[0] * T.shape[1] * 8 * 8 > 40 * 1024   # the global-memory table
+    o = oracle.Oracle(p, params)
+    Fo, So, ro = o.forces(3)
+    run = GpuRun(p, params=params)
+    run.build()
+    real = real_slots(p)
+    for flags in (ALL | nbk.NBK_PAIRLIST | nbk.NBK_CORRECTIONS, ALL | nbk.NBK_CORRECTIONS):
+        F, S, res, _ = run.eval(flags)
+        err = compare(F, S, res, Fo, So, ro, real)
+        print(f"beta {beta} cutoff {cutoff} flags={flags} " +
+              " ".join(f"{k}={v:.2e}" for k, v in err.items()))
+        assert err["force"] <= FORCE_RMS_TOL and err["slow"] <= FORCE_RMS_TOL, err
+        for k in ("energyVdw", "energyElec", "energySlow"):
+            assert err[k] <= ENERGY_TOL, (k, err)
+        assert err["virial"] <= VIRIAL_TOL and err["virialSlow"] <= VIRIAL_TOL, err
+        assert run.nb.pair_count() == ro["pairs"]
+    tl, ja, ex = run.nb.export_tile_lists()
+    keys = nbk.pairs_from_tile_lists(tl, ja, ex, p.atomStorageSize)
+    ref, _ = o.pairs()
+    assert np.array_equal(keys, ref)
+
+
 def test_pair_count(mixed):
     """The GPU's count of interacting pairs (the benchmark's work unit)
     equals the oracle's."""
