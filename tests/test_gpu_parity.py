@@ -74,19 +74,22 @@ def test_forces_mixed(mixed, corr):
     _check_forces(mixed, corr)
 
 
-@pytest.mark.parametrize("beta,cutoff,switch,pl", [(0.34, 10.0, 8.5, 11.5), (0.43, 8.0, 7.0, 9.5)])
-def test_forces_other_cutoffs(mixed, beta, cutoff, switch, pl):
+@pytest.mark.parametrize("beta,cutoff,switch,pl,global_table",
+                         [(0.34, 10.0, 8.5, 11.5, True), (0.43, 8.0, 7.0, 9.5, True),
+                          (PARAMS.ewaldcof, 12.0, 12.0, 13.5, False)])
+def test_forces_other_cutoffs(mixed, beta, cutoff, switch, pl, global_table):
     """Shorter cutoffs with the Ewald coefficients that a PME tolerance of
-    1e-6 gives for them, against the oracle with the same parameters: the
-    pair set, forces, energies and virials. With these the precise kernel's
-    slow-term table (136 and 186 rows) is too large for shared memory and is
-    read from global memory."""
+    1e-6 gives for them, and the benchmark's cutoff without LJ switching
+    (switchdist = cutoff), against the oracle with the same parameters: the
+    pair set, forces, energies and virials. With the shorter cutoffs the
+    precise kernel's slow-term table (136 and 186 rows) is too large for
+    shared memory and is read from global memory."""
     import dataclasses
     s, p, _ = mixed
     params = dataclasses.replace(PARAMS, ewaldcof=beta, cutoff=cutoff, switchdist=switch,
                                  pairlistdist=pl)
     T, _ = nbk.slow_table(beta, cutoff, pl)
-    assert T.shape[0] * T.shape[1] * 8 * 8 > 40 * 1024   # the global-memory table
+    assert (T.shape[0] * T.shape[1] * 8 * 8 > 40 * 1024) == global_table
     o = oracle.Oracle(p, params)
     Fo, So, ro = o.forces(3)
     run = GpuRun(p, params=params)
