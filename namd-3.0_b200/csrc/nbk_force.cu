@@ -390,14 +390,36 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
     float2 fix2 = f2(0.f), fiy2 = f2(0.f), fiz2 = f2(0.f);
     float2 fisx2 = f2(0.f), fisy2 = f2(0.f), fisz2 = f2(0.f);
 
+    // the next tile's mask word and j atom are loaded while the current tile
+    // is computed; the j-tile starts come 32 at a time (lane t holds tile
+    // jtFirst + 32 b + t) and are handed out by a shuffle
+    int jsBlock = 0;
+    unsigned maskNext = 0;
+    float4 xjNext = make_float4(0.f, 0.f, 0.f, 0.f);
+    int tyNext = 0;
     for (int jt = jtFirst; jt <= jtLast; ++jt) {
-      const int jstart = a.tileJatomStart[jt];
-      const unsigned mask = a.tileExcls[jt].excl[lane];
+      const int tb = (jt - jtFirst) & 31;
+      if (tb == 0) {
+        const int jtl = jt + lane;
+        jsBlock = jtl <= jtLast ? a.tileJatomStart[jtl] : 0;
+        const int js0 = __shfl_sync(0xffffffffu, jsBlock, 0);
+        maskNext = a.tileExcls[jt].excl[lane];
+        xjNext = a.xyzq[js0 + lane];
+        tyNext = a.vdwTypes[js0 + lane];
+      }
+      const int jstart = __shfl_sync(0xffffffffu, jsBlock, tb);
+      const unsigned mask = maskNext;
+      const float4 xj = xjNext;
+      const float tyj = __int_as_float(tyNext);
+      if (jt < jtLast && tb < 31) {
+        const int js1 = __shfl_sync(0xffffffffu, jsBlock, tb + 1);
+        maskNext = a.tileExcls[jt + 1].excl[lane];
+        xjNext = a.xyzq[js1 + lane];
+        tyNext = a.vdwTypes[js1 + lane];
+      }
       const unsigned stepMask = __reduce_or_sync(0xffffffffu, mask);
       unsigned live = 0;  // interacting pairs of this lane, TileExcl bit order
       if (stepMask != 0) {
-        const float4 xj = a.xyzq[jstart + lane];
-        const float tyj = __int_as_float(a.vdwTypes[jstart + lane]);
         // entry m holds (atom m & 31, atom (m & 31) ^ 16): one 8-byte load
         // gives both packed elements of an iteration
         const float2 ex = make_float2(xj.x, __shfl_xor_sync(0xffffffffu, xj.x, 16));
