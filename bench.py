@@ -952,8 +952,9 @@ def run_adjoint(args, rank, world, local_rank):
 def run_profile_case(args, local_rank):
     """The short fixed launch sequence that kernel captures run under ncu: the
     workload's system (seed 2), one tile-list build and pairlist evaluation,
-    then three steady E+V+S evaluations at launch shape (5, 1) with kernel
-    timing on. Prints the force and precise kernel times; no JSON line."""
+    then three steady E+V+S evaluations at the default launch shape (4, 1)
+    with kernel timing on. Prints the force and precise kernel times; no JSON
+    line."""
     import torch
     import nbk
     torch.cuda.set_device(local_rank)
@@ -965,7 +966,7 @@ def run_profile_case(args, local_rank):
     x = torch.from_numpy(packed.xyzq.copy()).cuda()
     nb.build_tile_lists(packed, xyzq=x)
     nb.force(packed, fl | nbk.NBK_PAIRLIST, xyzq=x)
-    nb.set_tuning(fl, 5, 1)
+    nb.set_tuning(fl, 4, 1)
     nb.set_kernel_timing(True)
     for _ in range(3):
         nb.force(packed, fl, xyzq=x)
