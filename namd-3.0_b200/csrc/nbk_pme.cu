@@ -102,12 +102,13 @@ __device__ __forceinline__ void gridCell(const float4 a, int K1, int K2, int K3,
 
 // One warp spreads 32 atoms: each lane computes its atom's weights into
 // shared memory, then the warp walks the atoms, its lanes covering the
-// order^3 grid points of one atom (x fastest, so neighbouring lanes add to
-// neighbouring addresses).
+// order^3 grid points of one atom (point p = lane + 32 h, x fastest, so
+// neighbouring lanes add to neighbouring addresses).
 template <int order>
 __global__ void __launch_bounds__(128) spreadKernel(int n, const float4* __restrict__ atoms, int K1,
                                                     int K2, int K3,
                                                     unsigned long long* __restrict__ grid) {
+  constexpr int kPts = order * order * order;
   __shared__ float s_th[4][3][order][32];
   __shared__ int s_i[4][3][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -134,18 +135,24 @@ __global__ void __launch_bounds__(128) spreadKernel(int n, const float4* __restr
     }
     __syncwarp();
     const int na = min(32, n - a0);
+    const int K12 = K1 * K2;  // grid indices below 2^31 (checked at creation)
     for (int m = 0; m < na; ++m) {
-      for (int p = lane; p < order * order * order; p += 32) {
-        const int x0 = p % order, y0 = (p / order) % order, z0 = p / (order * order);
-        int x = s_i[wib][0][m] + x0, y = s_i[wib][1][m] + y0, z = s_i[wib][2][m] + z0;
-        if (x >= K1) x -= K1;
-        if (y >= K2) y -= K2;
-        if (z >= K3) z -= K3;
-        const float v = s_th[wib][0][x0][m] * s_th[wib][1][y0][m] * s_th[wib][2][z0][m];
-        // v 2^32 is exact in FP32 (a power-of-two scaling), so this is the
-        // same integer as the FP64 product rounded to the nearest
-        const long long q = __float2ll_rn(v * kGridScale);
-        atomicAdd(&grid[x + (size_t)K1 * (y + (size_t)K2 * z)], (unsigned long long)q);
+      const int bx = s_i[wib][0][m], by = s_i[wib][1][m], bz = s_i[wib][2][m];
+#pragma unroll
+      for (int h = 0; h < (kPts + 31) / 32; ++h) {
+        const int p = lane + 32 * h;
+        if (kPts % 32 == 0 || p < kPts) {
+          const int x0 = p % order, y0 = (p / order) % order, z0 = p / (order * order);
+          int x = bx + x0, y = by + y0, z = bz + z0;
+          if (x >= K1) x -= K1;
+          if (y >= K2) y -= K2;
+          if (z >= K3) z -= K3;
+          const float v = s_th[wib][0][x0][m] * s_th[wib][1][y0][m] * s_th[wib][2][z0][m];
+          // v 2^32 is exact in FP32 (a power-of-two scaling), so this is the
+          // same integer as the FP64 product rounded to the nearest
+          const long long q = __float2ll_rn(v * kGridScale);
+          atomicAdd(&grid[x + K1 * y + K12 * z], (unsigned long long)q);
+        }
       }
     }
     __syncwarp();
@@ -280,8 +287,8 @@ struct GatherArgs {
 };
 
 // One thread per atom: the gradient of the interpolated potential, summed
-// over the order^3 points in a fixed order, then -q times the Cartesian
-// gradient.
+// over the order^3 points in a fixed order (along x first, then row by row),
+// then -q times the Cartesian gradient.
 template <int order>
 __global__ void gatherKernel(const __grid_constant__ GatherArgs a) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
@@ -293,6 +300,12 @@ __global__ void gatherKernel(const __grid_constant__ GatherArgs a) {
     bsplineThetaD<order>(wx, tx, dx);
     bsplineThetaD<order>(wy, ty, dy);
     bsplineThetaD<order>(wz, tz, dz);
+    const int K12 = a.K1 * a.K2;  // grid indices below 2^31 (checked at creation)
+    int xs[order];
+#pragma unroll
+    for (int x0 = 0; x0 < order; ++x0) xs[x0] = (ix + x0 >= a.K1) ? ix + x0 - a.K1 : ix + x0;
+    // per grid row (y0, z0): the x sums of theta_x g and dtheta_x g, then the
+    // row's y and z factors
     float f1 = 0.f, f2 = 0.f, f3 = 0.f;
 #pragma unroll 2
     for (int z0 = 0; z0 < order; ++z0) {
@@ -302,16 +315,17 @@ __global__ void gatherKernel(const __grid_constant__ GatherArgs a) {
       for (int y0 = 0; y0 < order; ++y0) {
         int y = iy + y0;
         if (y >= a.K2) y -= a.K2;
-        const float* row = a.grid + (size_t)a.K1 * (y + (size_t)a.K2 * z);
+        const float* row = a.grid + (a.K1 * y + K12 * z);
+        float sx = 0.f, sdx = 0.f;
 #pragma unroll
         for (int x0 = 0; x0 < order; ++x0) {
-          int x = ix + x0;
-          if (x >= a.K1) x -= a.K1;
-          const float g = __ldg(&row[x]);
-          f1 = fmaf(dx[x0] * ty[y0] * tz[z0], g, f1);
-          f2 = fmaf(tx[x0] * dy[y0] * tz[z0], g, f2);
-          f3 = fmaf(tx[x0] * ty[y0] * dz[z0], g, f3);
+          const float g = __ldg(&row[xs[x0]]);
+          sx = fmaf(tx[x0], g, sx);
+          sdx = fmaf(dx[x0], g, sdx);
         }
+        f1 = fmaf(sdx, ty[y0] * tz[z0], f1);
+        f2 = fmaf(sx, dy[y0] * tz[z0], f2);
+        f3 = fmaf(sx, ty[y0] * dz[z0], f3);
       }
     }
     const double q = -(double)at.w;
