@@ -9,6 +9,7 @@
 // time, ballot + popc place the survivors), and every list writes into a
 // slot range reserved on the host from the patch sizes, so the build never
 // overflows, never synchronises with the host and can be captured in a graph.
+#include <atomic>
 #include "nbk_internal.cuh"
 #include "nbk_launch.h"
 
@@ -338,14 +339,19 @@ __global__ void __launch_bounds__(128) refineKernel(const __grid_constant__ Forc
 
 cudaError_t launchRefine(const ForceArgs& a, int numSM, cudaStream_t st) {
   if (a.numListsHost <= 0) return cudaSuccess;
-  static int cachedBlocks = 0;
-  if (!cachedBlocks) {
+  // blocks per SM of this kernel (no dynamic shared memory, so the same on
+  // every device of one architecture); an atomic, as handles on several host
+  // threads may launch it at once
+  static std::atomic<int> cachedBlocks{0};
+  int blocks = cachedBlocks.load(std::memory_order_relaxed);
+  if (!blocks) {
     int nb = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, refineKernel, 128, 0);
     if (e != cudaSuccess) return e;
-    cachedBlocks = nb > 0 ? nb : 1;
+    blocks = nb > 0 ? nb : 1;
+    cachedBlocks.store(blocks, std::memory_order_relaxed);
   }
-  refineKernel<<<numSM * cachedBlocks, 128, 0, st>>>(a);
+  refineKernel<<<numSM * blocks, 128, 0, st>>>(a);
   return cudaGetLastError();
 }
 
