@@ -821,18 +821,19 @@ def batch_leg(steps, warmup, local_rank, rank=0):
            "product_one_handle_per_replica": {"value": plainv, "unit": "replica-evals/s",
                                               "ms_per_step": plain_ms / ksteps, "steps": ksteps},
            "speedup_vs_product_per_replica": batched / plainv}
-    ref = reference_batch(systems, params, warmup, ksteps, local_rank)
+    ref = reference_batch(systems, params, warmup, ksteps, local_rank, flush)
     if ref is not None:
         out["reference_one_instance_per_replica"] = ref
         out["speedup_vs_reference_plain_path"] = batched / ref["value"]
     return out
 
 
-def reference_batch(systems, params, warmup, ksteps, local_rank):
+def reference_batch(systems, params, warmup, ksteps, local_rank, flush):
     """The reference's plain GPU path on the batch: one CudaTileListKernel +
     CudaComputeNonbondedKernel instance per replica (its texture-table mode,
-    force + energy + virial + slow), steady steps back to back on one stream.
-    None when the reference harness is not built."""
+    force + energy + virial + slow), steady steps back to back on one stream,
+    L2 flushed before each step as for the batched arm. None when the
+    reference harness is not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import refgpu
     if not refgpu.available():
@@ -854,14 +855,19 @@ def reference_batch(systems, params, warmup, ksteps, local_rank):
     for _ in range(warmup):
         for r, _x in refs:
             r.eval(0, 1, 1, 1, None)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(rs)
-    for _ in range(ksteps):
-        for r, _x in refs:
-            r.eval(0, 1, 1, 1, None)
-    e1.record(rs)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1) / ksteps
+    # the same protocol as the batched arm: L2 flushed before every step,
+    # outside the events
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(ksteps)]
+    with torch.cuda.stream(rs):
+        for k in range(ksteps):
+            flush.zero_()
+            ev[k][0].record(rs)
+            for r, _x in refs:
+                r.eval(0, 1, 1, 1, None)
+            ev[k][1].record(rs)
+    rs.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / ksteps
     for r, _x in refs:
         r.set_stream(0)
     del refs
