@@ -17,8 +17,9 @@
 //   - on energy and virial evaluations it stores, per tile and lane, which of
 //     the lane's pairs interact (the live words).
 // preciseKernel: the electrostatic energies and the slow virial in FP64, from
-// the live words: per tile, the interacting pairs are compacted into a queue
-// and evaluated 32 at a time from FP64 geometry (see precisePass); its own
+// the live words: per tile, each lane walks a contiguous range of the tile's
+// interacting pairs straight from the live words and evaluates them from
+// FP64 geometry (see precisePass); its own
 // launch runs at higher occupancy than the register- and shared-memory-heavy
 // FP32 loop, which hides the FP64 dependency chains.
 #include "nbk_internal.cuh"
@@ -80,7 +81,7 @@ __device__ __forceinline__ void flushPrecise(long long* acc, int lane, long long
   npair = 0;
 }
 
-// FP64 geometry of one queued pair: d = x_j - x_i and the charge product.
+// FP64 geometry of one interacting pair: d = x_j - x_i and the charge product.
 struct PairTerms {
   double dx, dy, dz, qq;
 };
@@ -88,10 +89,9 @@ struct PairTerms {
 // The warp's atoms as the precise pass reads them: the list's i atoms in FP64
 // (shifted by the exact lattice translation) as two rows of 32 (x, y) and
 // (z, q) pairs, and the current j tile as it is stored (FP32 x, y, z, q, exact
-// in FP64). A queued pair reads two 16-byte entries of its i atom, mostly
-// broadcasts (lane-major queue order), and one of its j atom: the j reads
-// span the 512 bytes of the row, half of what FP64 rows would, and the four
-// conversions to FP64 cost less than the second load.
+// in FP64). A pair reads two 16-byte entries of its i atom and one of its j
+// atom: the j reads span the 512 bytes of the row, half of what FP64 rows
+// would, and the four conversions to FP64 cost less than the second load.
 struct Atoms64 {
   double2 ixy[kWarp], izq[kWarp];
   float4 j[kWarp];
@@ -184,36 +184,74 @@ __device__ __forceinline__ void precisePair(const PairTerms& u, const SlowTable&
   }
 }
 
-// Queue entry e of the precise pass as FP64 pair terms, from the warp's
-// atoms in shared memory. An entry past the end (e >= total) repeats entry 0,
-// a real pair (its atoms are distinct, so its distance is not 0), with
-// qq = 0, which contributes exact zeros.
-__device__ __forceinline__ void loadPair(const unsigned short* q, const int e, const int total,
-                                         const Atoms64& A, PairTerms& u) {
-  const bool valid = e < total;
-  const unsigned ent = q[valid ? e : 0];
-  const int i = ent & 31, j = (i + (ent >> 5)) & 31;
+// The FP64 pair terms of the pair (i, j = (i + t) & 31) from the warp's atoms
+// in shared memory; qq = 0 (exact zeros) when the lane has no pair left and
+// repeats its last one, a real interacting pair (so its distance is not 0).
+__device__ __forceinline__ void pairTerms(const Atoms64& A, const int i, const int t,
+                                          const bool valid, PairTerms& u) {
   const double2 ia = A.ixy[i], ib = A.izq[i];
-  const float4 jb = A.j[j];
+  const float4 jb = A.j[(i + t) & 31];
   u.dx = (double)jb.x - ia.x;
   u.dy = (double)jb.y - ia.y;
   u.dz = (double)jb.z - ib.x;
   u.qq = valid ? ib.y * (double)jb.w : 0.0;
 }
 
+// w without its r lowest set bits (r < popc(w)): the bits from the position p
+// of its (r + 1)-th set bit up, p being the largest position with at most r
+// set bits below it (a binary search over popc of w's low bits; p + step
+// stays below 32).
+__device__ __forceinline__ unsigned dropLowBits(const unsigned w, const int r) {
+  int p = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1)
+    if (__popc(w & ((1u << (p + step)) - 1u)) <= r) p += step;
+  return w & (0xffffffffu << p);
+}
+
+// One lane's walk over the tile's interacting pairs in lane-major order: the
+// owner lane i whose live bits w are not taken yet, and the last pair taken
+// (pi, pt).
+struct PairWalk {
+  int i, pi, pt;
+  unsigned w;
+};
+
+// Takes the lane's next pair when valid (the lowest bit of w; w is not 0 while
+// the lane has pairs left), then, once w is spent, moves on to the next lane
+// with live bits (nonEmpty: the lanes whose live word is not 0). Every lane
+// runs the shuffle; the source lane is in [0, 31].
+__device__ __forceinline__ void walkNext(PairWalk& s, const bool valid, const unsigned live,
+                                         const unsigned nonEmpty) {
+  if (valid) {
+    s.pt = __ffs(s.w) - 1;
+    s.pi = s.i;
+    s.w &= s.w - 1;
+  }
+  const int inext = __ffs(nonEmpty & (0xfffffffeu << s.i)) - 1;  // -1: none after i
+  const unsigned wn = __shfl_sync(0xffffffffu, live, inext & 31);
+  if (valid && s.w == 0u && inext >= 0) {
+    s.i = inext;
+    s.w = wn;
+  }
+}
+
 // The precise pass of one tile. live (per lane): bit t set when the pair
 // (i = lane, j = (lane + t) & 31) is an interacting pair (mask bit set and
 // FP32 r^2 below the cutoff, the classification the FP32 math used). The
-// warp compacts the tile's interacting pairs into a queue in shared memory
-// (entry = i | t << 5, lane-major order; at most 32 * 32 two-byte entries)
-// and processes them in FP64, two per lane per iteration
-// (entries e and e + 32: independent dependency chains) while more than 32
-// remain, then one. A pair's atoms come from the warp's FP64 rows (loadPair).
-// Every step is warp-synchronous and the sums depend only on the tile group.
+// tile's `total` interacting pairs, in lane-major order (by i, then t), are
+// split into 32 contiguous ranges of m = ceil(total / 32): lane k takes pairs
+// k m .. k m + m - 1 (the last lanes fewer or none). A lane finds the owner
+// of its first pair by a binary search over the lanes' inclusive counts
+// (shuffles), skips the owner's lower bits, and then walks the live words bit
+// by bit (walkNext), two pairs per iteration (independent dependency
+// chains). No queue is written. Each lane's sums take its pairs in a fixed
+// order, so they depend only on the tile's live words. A lane without pairs
+// repeats the tile's first pair with qq = 0.
 template <bool doEnergy, bool doVirial, bool doSlow, int kCopies>
 __device__ __forceinline__ void precisePass(const unsigned live, const int lane, const Atoms64& A,
-                                            unsigned short* q, const SlowTable& T,
-                                            const NbkConst& c, LaneSums& L, int& npair) {
+                                            const SlowTable& T, const NbkConst& c, LaneSums& L,
+                                            int& npair) {
   const int n = __popc(live);
   if (doEnergy) npair += n;
   int incl = n;
@@ -224,35 +262,43 @@ __device__ __forceinline__ void precisePass(const unsigned live, const int lane,
   }
   const int total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
   if (total == 0) return;  // warp-uniform
-  int pos = incl - n;
-  // two set bits per iteration (the loop runs up to popc(live) / 2 times)
-  for (unsigned w = live; w;) {
-    const int t0 = __ffs(w) - 1;
-    w &= w - 1;
-    q[pos] = (unsigned short)(lane | (t0 << 5));
-    if (w) {
-      const int t1 = __ffs(w) - 1;
-      w &= w - 1;
-      q[pos + 1] = (unsigned short)(lane | (t1 << 5));
-    }
-    pos += 2;
-  }
-  __syncwarp();
-  // two entries per lane per iteration while more than 32 remain, then one
-  int base = 0;
-  for (; total - base > kWarp; base += 2 * kWarp) {  // warp-uniform
-    PairTerms u[2];
+  const int m = (total + kWarp - 1) / kWarp;
+  const unsigned nonEmpty = __ballot_sync(0xffffffffu, live != 0u);
+  int e0 = lane * m;
+  const int cnt = min(m, max(0, total - e0));
+  if (e0 >= total) e0 = 0;
+  // owner of pair e0: the number of lanes whose inclusive count is <= e0
+  int owner = 0;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) loadPair(q, base + h * kWarp + lane, total, A, u[h]);
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int v = __shfl_sync(0xffffffffu, incl, owner + step - 1);
+    if (v <= e0) owner += step;
+  }
+  const int ownerExcl = __shfl_sync(0xffffffffu, incl - n, owner);
+  const unsigned ownerLive = __shfl_sync(0xffffffffu, live, owner);
+  PairWalk s;
+  s.i = owner;
+  s.w = dropLowBits(ownerLive, e0 - ownerExcl);
+  s.pi = owner;
+  s.pt = __ffs(s.w) - 1;
+  __syncwarp();  // the i rows and this j tile, written by the lanes, are visible
+  int k = 0;
+  for (; k + 1 < m; k += 2) {  // warp-uniform
+    PairTerms u[2];
+    walkNext(s, k < cnt, live, nonEmpty);
+    pairTerms(A, s.pi, s.pt, k < cnt, u[0]);
+    walkNext(s, k + 1 < cnt, live, nonEmpty);
+    pairTerms(A, s.pi, s.pt, k + 1 < cnt, u[1]);
 #pragma unroll
     for (int h = 0; h < 2; ++h) precisePair<doEnergy, doVirial, doSlow, kCopies>(u[h], T, c, lane, L);
   }
-  if (base < total) {  // warp-uniform
+  if (k < m) {  // warp-uniform
     PairTerms u;
-    loadPair(q, base + lane, total, A, u);
+    walkNext(s, k < cnt, live, nonEmpty);
+    pairTerms(A, s.pi, s.pt, k < cnt, u);
     precisePair<doEnergy, doVirial, doSlow, kCopies>(u, T, c, lane, L);
   }
-  __syncwarp();  // the queue and the j rows are consumed before they are written again
+  __syncwarp();  // the j rows are consumed before they are written again
 }
 
 // End of a tile group: the lanes' sums are reduced per quantity by a fixed
@@ -609,7 +655,6 @@ constexpr int kPreciseMinBlocks = 3;
 template <bool doEnergy, bool doVirial, bool doSlow, bool doBatch, int kCopies>
 __global__ void __launch_bounds__(kPreciseThreads, kPreciseMinBlocks)
     preciseKernel(const __grid_constant__ ForceArgs a) {
-  __shared__ unsigned short s_queue[kPreciseWarps][kWarp * kWarp];
   __shared__ Atoms64 s_atoms[kPreciseWarps];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -683,7 +728,7 @@ __global__ void __launch_bounds__(kPreciseThreads, kPreciseMinBlocks)
       if (__any_sync(0xffffffffu, live != 0u)) {
         // the i rows and this j tile are visible after the pass's first __syncwarp
         A.j[lane] = xj;
-        precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, A, s_queue[wib], T, a.c,
+        precisePass<doEnergy, doVirial, doSlow, kCopies>(live, lane, A, T, a.c,
                                                          lsum, npair);
       }
       if (((jt - tl.jtileStart + 1) & (kFoldTiles - 1)) == 0 || jt == tl.jtileEnd)
