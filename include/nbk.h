@@ -214,7 +214,7 @@ NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSi
  * cancel to 1e-4 of the sum of |pair energies| only to ~1e-5. The LJ energy
  * (FP32 per pair) and the fast virial (from the fixed-point forces) hold
  * ~3e-7. Cost, measured on a B200 at 92,224 atoms (34 M pairs): the FP64
- * energy kernel runs 0.197 ms after the 0.401 ms force kernel, so an
+ * energy kernel runs 0.195 ms after the 0.403 ms force kernel, so an
  * evaluation with NBK_ENERGY costs about 1.5x a forces-only one. */
 NBK_API int nbk_nonbonded_force(nbk_handle h, int atomStorageSize, unsigned flags,
                                 nbk_float3 lata, nbk_float3 latb, nbk_float3 latc,
