@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(kForceThreads, MINB)
           const float2 Y = pA[64];
           const float2 Z = pA[128];
           const float2 DX = add2(X, nXi), DY = add2(Y, nYi), DZ = add2(Z, nZi);
-          const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+          const float2 R2 = fma2(DZ, DZ, fma2(DX, DX, mul2(DY, DY)));  // dist2's order
           const bool aA = (mk & 1u) && (R2.x < c.cutoff2);
           const bool aB = (mk & 0x10000u) && (R2.y < c.cutoff2);
           if (!__any_sync(0xffffffffu, aA || aB)) continue;

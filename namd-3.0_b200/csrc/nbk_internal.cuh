@@ -76,22 +76,28 @@ struct ListSeed {
   int pad;
 };
 
-// Shift of the i atoms, offset . lattice, with the reference's operand order
-// (src/CudaComputeNonbondedKernel.cu:720-722) made explicit as FMAs so that
-// host and device agree bit for bit.
+// Shift of the i atoms, offset . lattice, as the reference's expression
+// o.x a + o.y b + o.z c (src/CudaComputeNonbondedKernel.cu:720-722) rounds
+// once contracted: the first product fused into the first sum, fma(o.x, a,
+// o.y b), then fma(o.z, c, that). Written out as FMAs so that host and device
+// agree bit for bit. (With an orthorhombic lattice only one term of each
+// component is not 0, and every order gives the same bits.)
 __device__ __forceinline__ float3 shiftOf(const float3 o, const float3 a, const float3 b,
                                           const float3 c) {
   float3 s;
-  s.x = __fmaf_rn(o.z, c.x, __fmaf_rn(o.y, b.x, __fmul_rn(o.x, a.x)));
-  s.y = __fmaf_rn(o.z, c.y, __fmaf_rn(o.y, b.y, __fmul_rn(o.x, a.y)));
-  s.z = __fmaf_rn(o.z, c.z, __fmaf_rn(o.y, b.z, __fmul_rn(o.x, a.z)));
+  s.x = __fmaf_rn(o.z, c.x, __fmaf_rn(o.x, a.x, __fmul_rn(o.y, b.x)));
+  s.y = __fmaf_rn(o.z, c.y, __fmaf_rn(o.x, a.y, __fmul_rn(o.y, b.y)));
+  s.z = __fmaf_rn(o.z, c.z, __fmaf_rn(o.x, a.z, __fmul_rn(o.y, b.z)));
   return s;
 }
 
-// r^2 of d = xj - xi with the operand order dx*dx + dy*dy + dz*dz contracted
-// left to right (src/CudaComputeNonbondedKernel.cu:1225-1230).
+// r^2 of d = xj - xi as the reference's dx*dx + dy*dy + dz*dz
+// (src/CudaComputeNonbondedKernel.cu:1225-1230) rounds once contracted the same
+// way: fma(dz, dz, fma(dx, dx, dy dy)). Its kernels list a pair whose r^2 is
+// 182.249985 in this order and exactly plcutoff^2 = 182.25 in the order
+// fma(dz, dz, fma(dy, dy, dx dx)) (a triclinic test cell).
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
-  return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+  return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
 // erfc(x) = t P(t) exp(-x^2), t = 1/(1 + p x): Hastings' rational form (the

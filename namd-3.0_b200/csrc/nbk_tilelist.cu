@@ -297,7 +297,7 @@ __global__ void __launch_bounds__(128) refineKernel(const __grid_constant__ Forc
           const float2 DX = add2(make_float2(P0.x, P0.y), nXi);
           const float2 DY = add2(make_float2(P0.z, P0.w), nYi);
           const float2 DZ = add2(make_float2(P1.x, P1.y), nZi);
-          const float2 R2 = fma2(DZ, DZ, fma2(DY, DY, mul2(DX, DX)));
+          const float2 R2 = fma2(DZ, DZ, fma2(DX, DX, mul2(DY, DY)));  // dist2's order
           const float2 C = add2(R2, nPlc2);  // negative: within the pairlist cutoff
           const float2 DI = add2(make_float2(P1.z, P1.w), nIi);
           const float2 W = fma2(DI, DI, nT);  // negative: within the maxdiff window

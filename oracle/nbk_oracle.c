@@ -10,7 +10,9 @@
  *     (i in patch1, j in patch2; j after i in slot order for a self compute)
  *     is listed iff its FP32 distance^2, formed with the reference's operand
  *     order (shift = offset . lattice; dx = xj - (xi + shift);
- *     r2 = dx*dx + dy*dy + dz*dz, contracted to FMAs left to right), is below
+ *     r2 = dx*dx + dy*dy + dz*dz, each sum contracted as the reference's
+ *     compiled kernels round it: the first product fused into the first sum,
+ *     fma(dz, dz, fma(dx, dx, dy*dy)), and likewise the shift), is below
  *     the FP32 pairlist cutoff^2, the pair is not a full exclusion, and at
  *     least one atom is free            (src/CudaComputeNonbondedKernel.cu:720-750,
  *                                        1225-1249; src/CudaTileListKernel.cu:405-548)
@@ -74,14 +76,14 @@ static inline void shift_f32(const oracle_system* s, int c, float* sh) {
   const float ox = s->computeOffset[3 * c], oy = s->computeOffset[3 * c + 1],
               oz = s->computeOffset[3 * c + 2];
   const float* L = s->lattice;
-  for (int d = 0; d < 3; ++d) sh[d] = fmaf(oz, L[6 + d], fmaf(oy, L[3 + d], ox * L[d]));
+  for (int d = 0; d < 3; ++d) sh[d] = fmaf(oz, L[6 + d], fmaf(ox, L[d], oy * L[3 + d]));
 }
 
 static inline float r2_f32(const float* xi_shifted, const float* xj) {
   const float dx = xj[0] - xi_shifted[0];
   const float dy = xj[1] - xi_shifted[1];
   const float dz = xj[2] - xi_shifted[2];
-  return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+  return fmaf(dz, dz, fmaf(dx, dx, dy * dy));
 }
 
 static inline int excluded(const oracle_system* s, int i, int j) {
@@ -103,7 +105,7 @@ static long long compute_pairs(const oracle_system* s, int c, unsigned long long
   const int* P2 = s->patches + 4 * p2;
   float sh[3];
   shift_f32(s, c, sh);
-  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[1], sh[1], sh[0] * sh[0])) > 0.0f);
+  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[0], sh[0], sh[1] * sh[1])) > 0.0f);
   const int self = (p1 == p2) && zeroShift;
   long long n = 0, ne = 0;
   for (int a = 0; a < P1[0]; ++a) {
@@ -233,7 +235,7 @@ static void nonbonded_compute(const oracle_system* s, const pair_consts* k, int 
   const int* P2 = s->patches + 4 * p2;
   float sh[3];
   shift_f32(s, c, sh);
-  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[1], sh[1], sh[0] * sh[0])) > 0.0f);
+  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[0], sh[0], sh[1] * sh[1])) > 0.0f);
   const int self = (p1 == p2) && zeroShift;
   /* FP64 shift from the FP32 offsets (the exact lattice translation) */
   double shd[3];
@@ -283,9 +285,9 @@ static void correction_tuple(const oracle_system* s, const pair_consts* k, const
   const float* xj = s->xyzq + 4 * (size_t)t->j;
   const float* L = s->lattice;
   float shf[3];
-  for (int d = 0; d < 3; ++d) shf[d] = fmaf(t->oz, L[6 + d], fmaf(t->oy, L[3 + d], t->ox * L[d]));
+  for (int d = 0; d < 3; ++d) shf[d] = fmaf(t->oz, L[6 + d], fmaf(t->ox, L[d], t->oy * L[3 + d]));
   const float xf = xi[0] + shf[0] - xj[0], yf = xi[1] + shf[1] - xj[1], zf = xi[2] + shf[2] - xj[2];
-  const float r2f = fmaf(zf, zf, fmaf(yf, yf, xf * xf));
+  const float r2f = fmaf(zf, zf, fmaf(xf, xf, yf * yf));
   if (!(r2f < s->cutoff2f)) return;
   double shd[3], dij[3];
   for (int a = 0; a < 3; ++a) {
@@ -526,7 +528,7 @@ static double adjoint_compute(const oracle_system* s, const pair_consts* k, int 
   const int* P2 = s->patches + 4 * p2;
   float sh[3];
   shift_f32(s, c, sh);
-  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[1], sh[1], sh[0] * sh[0])) > 0.0f);
+  const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[0], sh[0], sh[1] * sh[1])) > 0.0f);
   const int self = (p1 == p2) && zeroShift;
   double shd[3];
   for (int a = 0; a < 3; ++a)
@@ -661,7 +663,7 @@ int oracle_near_cutoff(const oracle_system* s, int slot, float tol) {
     const int* P2 = s->patches + 4 * p2;
     float sh[3];
     shift_f32(s, c, sh);
-    const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[1], sh[1], sh[0] * sh[0])) > 0.0f);
+    const int zeroShift = !(fmaf(sh[2], sh[2], fmaf(sh[0], sh[0], sh[1] * sh[1])) > 0.0f);
     const int self = (p1 == p2) && zeroShift;
     for (int a = 0; a < P1[0]; ++a) {
       const int i = P1[2] + a;

@@ -15,8 +15,10 @@ import pytest
 
 import nbk
 import oracle
+import refgpu
 from helpers import (ALL, ENERGY_TOL, FORCE_RMS_TOL, PARAMS, VIRIAL_TOL, GpuRun,
-                     PackedVariant, compare, mixed_box, real_slots)
+                     PackedVariant, compare, mixed_box, real_slots, reference_pairs, rel,
+                     rms_rel, unordered_keys)
 
 pytestmark = pytest.mark.gpu
 
@@ -85,3 +87,35 @@ def test_triclinic_forces_energies_virials(triclinic, corr):
         assert err["energyVdw"] <= ENERGY_TOL, err
         assert err["energyElec"] <= ENERGY_TOL and err["energySlow"] <= ENERGY_TOL, err
         assert err["virial"] <= VIRIAL_TOL and err["virialSlow"] <= VIRIAL_TOL, err
+
+
+@pytest.mark.skipif(not refgpu.available(), reason="reference kernels not built (oracle/ref_gpu)")
+def test_triclinic_reference_kernels(triclinic):
+    """The reference's own CudaTileListKernel and CudaComputeNonbondedKernel on
+    the same sheared cell: their refined pair set equals the oracle's, and their
+    direct-math fast forces, LJ energy and virial (the reference allows direct
+    math only without slow forces) agree with the oracle as they do on the
+    orthorhombic systems. This pins the oracle's triclinic shifts and virial to
+    the reference, not only to the product."""
+    s, p, o = triclinic
+    xyzq = np.ascontiguousarray(p.xyzq)
+    tab = refgpu.RefGpu(PARAMS, s.lj_table(), do_table=1)  # its mode with slow forces
+    tab.setup(p)
+    ku, nexcl = reference_pairs(tab, xyzq, p.atomStorageSize)
+    ok, nex = o.pairs()
+    assert np.array_equal(ku, unordered_keys(ok, p.atomStorageSize))
+    assert nexcl == nex
+    del tab
+    ref = refgpu.RefGpu(PARAMS, s.lj_table(), do_table=0)
+    ref.setup(p)
+    Fo, So, ro = o.forces(1)
+    real = real_slots(p)
+    for pl in (1, 0):
+        ref.eval(pl, 1, 1, 0, xyzq)
+        F, S, ve = ref.results()
+        e = dict(force=rms_rel(F[real, :3].astype(np.float64), Fo[real]),
+                 energyVdw=rel(ve[18], ro["energyVdw"]),
+                 virial=rms_rel(ve[:9].reshape(3, 3), ro["virial"]))
+        print(f"reference direct math, triclinic, pairlist={pl}: "
+              + " ".join(f"{k}={v:.2e}" for k, v in e.items()))
+        assert e["force"] <= FORCE_RMS_TOL and e["virial"] <= 1e-5 and e["energyVdw"] <= 1e-5, e
