@@ -183,7 +183,10 @@ NBK_API int nbk_update_vdw_types_excl(nbk_handle h, int atomStorageSize, const i
  * maxTileListLen, or maxTileListLen >= 65536, returns NBK_ERR_OVERFLOW and sets
  * tilesSizeExceeded in the TileListStat (the reference's tilesSizeExceeded,
  * src/CudaTileListKernel.cu:505-509; it reallocates and rebuilds, the caller
- * here rebuilds with a larger maxTileListLen). */
+ * here rebuilds with a larger maxTileListLen). lata, latb, latc are the
+ * general (triclinic) lattice vectors, as the reference takes them; a compute's
+ * shift is offsetXYZ.x lata + offsetXYZ.y latb + offsetXYZ.z latc, rounded in
+ * FP32 as the reference's kernels round it. */
 NBK_API int nbk_build_tile_lists(nbk_handle h, int numPatches, int atomStorageSize,
                                  int maxTileListLen, nbk_float3 lata, nbk_float3 latb,
                                  nbk_float3 latc, const nbk_patch_record* h_patches,
